@@ -1,0 +1,416 @@
+"""Benchmark: GROG fused gridding forward + adjoint (samples*coils/s) on B200.
+
+Workload (the 3-D roofline configuration): 192^3 grid, kooshball trajectory
+of 20,000 spokes x 384 samples (golden means), 12 coils (32 seeded Gaussian
+coils compressed to 12 by PCA of the calibration block), kernel width 2
+sphere (kw = 4), shift table precision 1 (11^3 entries), oversampling 1.
+A step is one fused forward (interpolate + EGROG weight + scatter onto the
+grid) plus one adjoint (gather + conjugate-transposed shift) over the whole
+trajectory.  value = N_samples * C / step time, inputs resident in HBM
+(737 MB of samples, 679 MB of grid: both larger than L2, so no flush needed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the path
+shards by reconstruction; no data-path collective) and the max time over
+ranks is reported.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+N_SPOKES, N_READOUT, GRID_N, N_COILS_RAW, N_COILS = 20000, 384, 192, 32, 12
+CPU_SAMPLE_SPOKES = 2000
+METRIC = "GROG samples*coils/s fwd+adj (3-D kooshball 192^3, C=12)"
+UNIT = "samples*coils/s"
+
+
+def _dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def _peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:  # noqa: BLE001
+            pass
+    return 6650.0, "fallback"
+
+
+def _profile_traffic(kernel: str):
+    """DRAM bytes per launch of ``kernel`` recorded from an ncu capture in profiles/."""
+    for f in sorted((REPO / "profiles").glob("*.md")):
+        for line in f.read_text().splitlines():
+            m = re.match(rf"\s*[-*]?\s*traffic_per_launch\[{re.escape(kernel)}\]\s*[:=]\s*([0-9.eE+]+)", line)
+            if m:
+                return float(m.group(1)), f.name
+    return None, None
+
+
+def build_workload(device, seed: int = 1001):
+    """Plan + table + device-resident data for the 3-D configuration."""
+    import torch
+
+    from pygrog_b200.calib import GrogInterpolator
+    from pygrog_b200.workloads import kooshball
+
+    coords = kooshball(N_SPOKES, N_READOUT, GRID_N / 2.0)
+    g = GrogInterpolator(shape=(GRID_N,) * 3, coords=coords, oversamp=1.0, kernel_width=2,
+                         kernel_shape="sphere", device=device)
+    acr = make_acr3d(device, seed)
+    g.calc_interp_table(acr, lamda=0.01, precision=1)
+    gen = torch.Generator(device=device).manual_seed(seed)
+    N = N_SPOKES * N_READOUT
+    data = torch.randn(1, N_COILS, N, dtype=torch.complex64, device=device, generator=gen)
+    return g, coords, acr, data
+
+
+def make_acr3d(device, seed: int):
+    """Centre 24^3 of the k-space of 32 Gaussian-coil images of a random
+    ellipsoid phantom, PCA-compressed to 12 virtual coils (host FP64 SVD)."""
+    import torch
+
+    n = GRID_N
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    ax = torch.linspace(-1, 1, n, device=device)
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    ph = torch.zeros(n, n, n, device=device)
+    for _ in range(10):
+        c = (torch.rand(3, generator=gen) * 1.2 - 0.6).tolist()
+        a = (torch.rand(3, generator=gen) * 0.35 + 0.05).tolist()
+        v = float(torch.rand(1, generator=gen) * 0.9 + 0.1)
+        m = ((x - c[0]) / a[0]) ** 2 + ((y - c[1]) / a[1]) ** 2 + ((z - c[2]) / a[2]) ** 2 <= 1
+        ph = ph + v * m
+    acr = torch.empty(N_COILS_RAW, 24, 24, 24, dtype=torch.complex64)
+    lo = (n - 24) // 2
+    for k in range(N_COILS_RAW):
+        u = torch.randn(3, generator=gen)
+        u = (0.7 * u / u.norm()).tolist()
+        bump = torch.exp(-((x - u[0]) ** 2 + (y - u[1]) ** 2 + (z - u[2]) ** 2) / (2 * 0.7**2))
+        phase = float(torch.rand(1, generator=gen)) * 2 * math.pi
+        img = (ph * bump).to(torch.complex64) * complex(math.cos(phase), math.sin(phase))
+        k3 = torch.fft.fftshift(torch.fft.fftn(torch.fft.ifftshift(img), norm="ortho"))
+        acr[k] = k3[lo:lo + 24, lo:lo + 24, lo:lo + 24].cpu()
+    flat = acr.reshape(N_COILS_RAW, -1).to(torch.complex128)
+    u, s, vh = torch.linalg.svd(flat, full_matrices=False)
+    comp = u[:, :N_COILS].conj().T  # (12, 32)
+    return (comp @ flat).reshape(N_COILS, 24, 24, 24).to(torch.complex64).numpy()
+
+
+def cpu_baseline(coords, acr, spokes: int):
+    """Reference CPU implementation timed on a bounded sample of the trajectory."""
+    from oracle.ref_cpu import ReferenceCPU
+
+    sub = coords[:spokes]
+    rc = ReferenceCPU((GRID_N,) * 3, sub, 1.0, 2, "sphere", acr, 1, 0.01)
+    rng = np.random.default_rng(7)
+    data = (rng.standard_normal((N_COILS, sub.shape[0] * sub.shape[1]))
+            + 1j * rng.standard_normal((N_COILS, sub.shape[0] * sub.shape[1]))).astype(np.complex64)
+    rc.time_step(data, 1)  # warm-up
+    dt = rc.time_step(data, 2)
+    v = sub.shape[0] * sub.shape[1] * N_COILS / dt
+    return {
+        "value": v,
+        "unit": UNIT,
+        "cores": rc.threads,
+        "kind": rc.kind,
+        "sample": f"{spokes} of {N_SPOKES} spokes x {N_READOUT} samples, C={N_COILS}, fwd+adj, best of 2",
+    }
+
+
+def run_reference_arm(args):
+    ws, rank, local = _dist_env()
+    if rank != 0:
+        return 0
+    from pygrog_b200.workloads import kooshball
+
+    coords = kooshball(N_SPOKES, N_READOUT, GRID_N / 2.0)
+    rng = np.random.default_rng(1001)
+    acr = (rng.standard_normal((N_COILS, 24, 24, 24)) + 1j * rng.standard_normal((N_COILS, 24, 24, 24))).astype(np.complex64)
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            dev = torch.device("cuda", local)
+            acr = make_acr3d(dev, 1001)
+    except Exception:  # noqa: BLE001
+        pass
+    from oracle.ref_cpu import ReferenceCPU
+
+    spokes = CPU_SAMPLE_SPOKES
+    sub = coords[:spokes]
+    rc = ReferenceCPU((GRID_N,) * 3, sub, 1.0, 2, "sphere", acr, 1, 0.01)
+    data = (rng.standard_normal((N_COILS, sub.shape[0] * sub.shape[1]))
+            + 1j * rng.standard_normal((N_COILS, sub.shape[0] * sub.shape[1]))).astype(np.complex64)
+    for _ in range(max(args.warmup, 1)):
+        rc.time_step(data, 1)
+    times = [rc.time_step(data, 1) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    v = sub.shape[0] * sub.shape[1] * N_COILS / t
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64",
+        "data": "synthetic",
+        "config": {"workload": "grog3d_kooshball_192c12_fwd_adj", "grid": [GRID_N] * 3,
+                   "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS, "kw": 4, "precision": 1,
+                   "reference_sample_spokes": spokes},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": rc.threads, "kind": rc.kind,
+                         "sample": f"{spokes} of {N_SPOKES} spokes per step (reference CPU path, "
+                                   f"{rc.threads} threads)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    ws, rank, local = _dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    g, coords, acr, data = build_workload(dev)
+    bp = g._brick(0)
+    G = int(np.prod(g.plan.grid_shape))
+    B, C, N = data.shape
+    kgrid = torch.empty(B, C, G, dtype=torch.complex64, device=dev)
+    out = torch.empty(B, C, N, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(evs=None):
+        if evs is not None:
+            evs[0].record(stream)
+        bp.grid_forward(data, g._table_d, kgrid)
+        if evs is not None:
+            evs[1].record(stream)
+        bp.grid_adjoint(kgrid, g._table_h_d, out)
+        if evs is not None:
+            evs[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    fwd_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    adj_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    ms = total_ms / args.steps
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ws * N * C * B / (ms / 1e3)
+
+    # algorithmic bytes per launch (both directions): samples + per-replica metadata + grid
+    alg_bytes = N * C * 8 * B + bp.n_valid * 12 + G * C * 8 * B
+    dom = "grog_grid_kernel" if fwd_ms >= adj_ms else "grog_degrid_kernel"
+    dom_ms = max(fwd_ms, adj_ms)
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    traffic, tsrc = _profile_traffic(dom)
+    n_launch = (2 if bp.split_bricks.numel() else 1) + (1 if (not bp.multi and bp.zero_src.numel()) else 0) + 1
+
+    # end to end through the public API with host buffers (pinned)
+    e2e = None
+    if args.e2e_steps > 0:
+        x_host = data[0].cpu().reshape(C, N_SPOKES, N_READOUT).pin_memory()
+        torch.cuda.synchronize(dev)
+        kg = g.grid(x_host)
+        g.degrid(kg)
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            kg = g.grid(x_host)  # H2D samples, fused forward, D2H grid
+            y = g.degrid(kg)  # H2D grid, fused adjoint, D2H samples
+            torch.cuda.synchronize(dev)
+            ts.append(time.perf_counter() - t0)
+        t_e2e = float(np.median(ts))
+        e2e = {
+            "value": ws * N * C / t_e2e,
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(x_host.numel() * 8 + kg.numel() * 8),
+            "d2h_bytes_per_step": int(kg.numel() * 8 + y.numel() * 8),
+            "api": "GrogInterpolator.grid(pinned host tensor) + GrogInterpolator.degrid(host tensor)",
+        }
+
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline(coords, acr, CPU_SAMPLE_SPOKES)
+            except Exception as exc:  # noqa: BLE001
+                cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
+                       "sample": f"failed: {exc}"}
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64",
+            "data": "synthetic",
+            "config": {
+                "workload": "grog3d_kooshball_192c12_fwd_adj",
+                "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
+                "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
+                "n_valid_replicas": bp.n_valid, "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
+                "parallelism": f"replicas x{ws}",
+            },
+            "fwd_ms": fwd_ms,
+            "adj_ms": adj_ms,
+            "roofline": {
+                "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "algorithmic_bytes": alg_bytes,
+                "traffic": traffic, "traffic_source": tsrc,
+            },
+            "clocks": clocks,
+            "gpu_launches": n_launch * args.steps,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,204 @@
+/*
+ * pygrog_b200.h -- C ABI of the sm_100a GROG gridding hot path.
+ *
+ * Every entry point takes plain device pointers, element counts and a
+ * cudaStream_t (passed as void*), launches asynchronously on that stream,
+ * allocates nothing, and returns a status code (PGB_OK == 0).  On failure,
+ * pgb_last_error() returns a human-readable message for the calling thread.
+ *
+ * Complex data are interleaved (re, im) pairs: complex64 = float2,
+ * complex128 = double2.  `dtype` selects PGB_C64 (complex64 data with float32
+ * weights) or PGB_C128 (complex128 data with float64 weights).
+ *
+ * Reference interfaces replaced (FiRMLAB-Pisa/pygrog):
+ *   csrc/torch/module.cpp:54-87 binds seven functions with pybind11; each
+ *   pgb_* entry point below that carries a "replaces" line is its drop-in.
+ *   The remaining entry points are the fused operators of the GROG path
+ *   (plan build, fused grid/degrid, SparseFFT/Toeplitz pointwise stages and
+ *   the device-side CG scalars), each citing the reference Python it
+ *   replaces.
+ */
+#ifndef PYGROG_B200_H
+#define PYGROG_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PGB_API __attribute__((visibility("default")))
+#else
+#define PGB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define PGB_OK 0
+#define PGB_ERR_INVALID 1     /* bad size / shape / pointer               */
+#define PGB_ERR_DTYPE 2       /* unsupported dtype code                   */
+#define PGB_ERR_CUDA 3        /* kernel launch or CUDA runtime failure    */
+#define PGB_ERR_UNSUPPORTED 4 /* e.g. coil count above the kernel limit   */
+#define PGB_ERR_RANGE 5       /* index or size beyond a documented limit  */
+
+/* ---- dtype codes ----------------------------------------------------- */
+#define PGB_C64 0  /* complex64 data, float32 weights  */
+#define PGB_C128 1 /* complex128 data, float64 weights */
+
+/* Message for the last failing call on this host thread ("" if none). */
+PGB_API const char* pgb_last_error(void);
+/* Library version string. */
+PGB_API const char* pgb_version(void);
+
+/* =====================================================================
+ * L0: the seven native functions of the reference extension
+ * ===================================================================== */
+
+/* out[n,b,co] = sum_ci kernel[idx[n],co,ci] * data[n,b,ci]
+ * data (N,B,C), idx (N,) int64, kernel (K,C,C), out (N,B,C).
+ * idx outside [0,K) yields zeros.
+ * replaces: grog_interpolate, csrc/torch/grog_interp.cpp:112-149 and
+ *           csrc/torch/grog_interp_cuda.cu:64-106 */
+PGB_API int pgb_grog_interpolate(const void* data, const int64_t* idx, const void* kernel,
+                         void* out, int64_t N, int64_t B, int64_t C, int64_t K,
+                         int dtype, void* stream);
+
+/* grid[idx[i]] += w[i] * data[i] (in place); indices outside [0,G) skipped.
+ * Sorted indices are fastest but not required.
+ * replaces: scatter_add, csrc/torch/sparse_ops.cpp:233-267,
+ *           csrc/torch/sparse_ops_cuda.cu:47-63,149-173 */
+PGB_API int pgb_scatter_add(void* grid, int64_t G, const void* data, const int64_t* idx,
+                    const void* w, int64_t N, int dtype, void* stream);
+
+/* Same result as pgb_scatter_add; uses the caller's bin layout
+ * (bin_starts (n_bins+1,) int64 offsets into sorted idx, bins of bin_size
+ * cells) to accumulate each bin in shared memory.
+ * replaces: scatter_add_binned, csrc/torch/sparse_ops.cpp:299-340,
+ *           csrc/torch/sparse_ops_cuda.cu:79-120,175-201 */
+PGB_API int pgb_scatter_add_binned(void* grid, int64_t G, const void* data,
+                           const int64_t* idx, const void* w, int64_t N,
+                           const int64_t* bin_starts, int64_t n_bins,
+                           int64_t bin_size, int dtype, void* stream);
+
+/* out[i] = w[i] * grid[idx[i]] (0 for idx outside [0,G)).
+ * replaces: gather, csrc/torch/sparse_ops.cpp:269-297,
+ *           csrc/torch/sparse_ops_cuda.cu:126-143,203-230 */
+PGB_API int pgb_gather(const void* grid, int64_t G, const int64_t* idx, const void* w,
+               void* out, int64_t N, int dtype, void* stream);
+
+/* psf[idx[i]] += w_sq[i] (real psf, float32 or float64 by dtype).
+ * replaces: psf_scatter_scalar, csrc/torch/toep_psf.cpp:242-274,
+ *           csrc/torch/toep_psf_cuda.cu:41-76 */
+PGB_API int pgb_psf_scatter_scalar(void* psf, int64_t G, const int64_t* idx,
+                           const void* w_sq, int64_t N, int dtype, void* stream);
+
+/* psf[idx[i],l,l'] += w_sq[i] * conj(b[i,l]) * b[i,l']; psf (G,M,M) complex,
+ * basis_per_sample (N,M) complex.
+ * replaces: psf_scatter_outer, csrc/torch/toep_psf.cpp:276-323,
+ *           csrc/torch/toep_psf_cuda.cu:83-133 */
+PGB_API int pgb_psf_scatter_outer(void* psf, int64_t G, int64_t M, const int64_t* idx,
+                          const void* w_sq, const void* basis_per_sample,
+                          int64_t N, int dtype, void* stream);
+
+/* psf[idx[i],k,k'] += w_sq[i] * conj(B[k,t_i]) * B[k',t_i]; psf (G,K,K),
+ * basis (K,T), time_index (N,) int64 (outside [0,T) skipped).
+ * replaces: psf_scatter_outer_basis, csrc/torch/toep_psf.cpp:325-367,
+ *           csrc/torch/toep_psf_cuda.cu:138-193 */
+PGB_API int pgb_psf_scatter_outer_basis(void* psf, int64_t G, int64_t K,
+                                const int64_t* idx, const void* w_sq,
+                                const void* basis, int64_t T,
+                                const int64_t* time_index, int64_t N, int dtype,
+                                void* stream);
+
+/* =====================================================================
+ * GROG plan construction (float32, bit-exact integer keys)
+ * ===================================================================== */
+
+/* Per-replica geometry of _create_plan_single (calib/_grog.py:1125-1212)
+ * for one trajectory.  coords_scaled (npts, ndim) float32 are the rescaled
+ * coordinates; offsets (kw, ndim) int32.  Writes, for r = n*kw + j:
+ *   target_idx[r] int64 flat cell (-1 when out of bounds or |d|>0.5),
+ *   distances[r*ndim + d] float32, gauss[r] float32 (0 when invalid).
+ * shape/grid_shape/origins/grid_steps are per axis (ndim <= 3). */
+PGB_API int pgb_plan_geometry(const float* coords_scaled, int64_t npts, int ndim,
+                      const int32_t* offsets, int kw, const int64_t* grid_shape,
+                      const float* origins, const float* grid_steps,
+                      int64_t* target_idx, float* distances, float* gauss,
+                      void* stream);
+
+/* gauss_sum[target] += (double)gauss (valid replicas); EGROG normalisation,
+ * calib/_grog.py:1203-1206. */
+PGB_API int pgb_plan_gauss_sum(const int64_t* target_idx, const float* gauss, int64_t R,
+                       double* gauss_sum, int64_t G, void* stream);
+
+/* weights[r] = gauss[r] / (float)max(gauss_sum[t], 1e-12) for valid r, else 0;
+ * calib/_grog.py:1208-1212. */
+PGB_API int pgb_plan_weights(const int64_t* target_idx, const float* gauss,
+                     const double* gauss_sum, int64_t R, float* weights,
+                     void* stream);
+
+/* Shift quantisation of calc_interp_table (calib/_grog.py:406-417):
+ *   i_d = rint((radius + rint(d*pfac)/pfac) / stepsize)
+ *   idx = clamp(sum_d (int32) rint(i_d * nsteps^d), 0, K-1)
+ * all in float32 with IEEE division (pfac, stepsize given as float32). */
+PGB_API int pgb_plan_quantize(const float* distances, int64_t R, int ndim, float radius,
+                      float pfac, float stepsize, int nsteps, int64_t K,
+                      int64_t* interp_idx, void* stream);
+
+/* =====================================================================
+ * Fused GROG operator (interpolate + weight + scatter, and its adjoint)
+ * ===================================================================== */
+
+/* Brick work plan shared by the fused kernels.  Valid replicas are sorted
+ * by (brick, cell); per replica:
+ *   rep_src  int32   source sample index,
+ *   rep_meta uint32  table entry (low 20 bits) | cell-in-brick << 20,
+ *   rep_w    float32 replica weight.
+ * work (n_work, 4) int32 rows: {brick, begin, end, split}; split=1 marks a
+ * chunk of a brick shared by several chunks.  Bricks are (bz,by,bx) cells
+ * (2-D grids use bz=1, grid_shape[0]=1). */
+typedef struct pgb_brick_plan {
+  const int32_t* rep_src;
+  const uint32_t* rep_meta;
+  const float* rep_w;
+  const int32_t* work;
+  int32_t n_work;
+  int32_t gz, gy, gx;       /* grid extent per axis (2-D: gz = 1)      */
+  int32_t bz, by, bx;       /* brick extent per axis                   */
+  int32_t nbz, nby, nbx;    /* bricks per axis                         */
+  const int32_t* split_bricks; /* bricks touched by split chunks     */
+  int32_t n_split_bricks;
+} pgb_brick_plan;
+
+/* Forward: grid[b,c,cell] = sum_{r->cell} w_r * (T[e_r] @ data[b,:,src_r])[c]
+ * data (B,C,N) complex64, grid (B,C,G) complex64, table (K,C,C) complex64.
+ * Every grid cell is written.  Replaces interpolate(grid=True),
+ * calib/_grog.py:437-555,668-695,736-902 (replicate, grog_interpolate,
+ * pre_weights, per-coil scatter_add). C <= 32. */
+PGB_API int pgb_grog_grid(const void* data, int64_t N, void* grid, int64_t G,
+                  const void* table, int64_t K, int64_t C, int64_t B,
+                  const pgb_brick_plan* plan, void* stream);
+
+/* Adjoint: out[b,:,n] = sum_{r: src_r=n} w_r * T[e_r]^H @ grid[b,:,cell_r]
+ * table_h (K,C,C) holds the conjugate transposes of the table.
+ * `accumulate` = 0 when every sample has at most one valid replica (plain
+ * stores; samples listed in zero_src (n_zero) are zeroed), 1 otherwise
+ * (out is zeroed then accumulated atomically).  No reference counterpart:
+ * the G^H adjoint of interpolate(grid=True) restated from its definition. */
+PGB_API int pgb_grog_degrid(const void* grid, int64_t G, void* out, int64_t N,
+                    const void* table_h, int64_t K, int64_t C, int64_t B,
+                    const pgb_brick_plan* plan, int accumulate,
+                    const int32_t* zero_src, int64_t n_zero, void* stream);
+
+/* Replica expansion of interpolate() (calib/_grog.py:668-695):
+ * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]
+ * data (B,C,N), out (B,C,N*kw); entries outside [0,K) give 0. C <= 32. */
+PGB_API int pgb_grog_expand(const void* data, int64_t N, int kw, const int64_t* interp_idx,
+                    const void* table, int64_t K, int64_t C, int64_t B, void* out,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYGROG_B200_H */

@@ -1,0 +1,142 @@
+"""ctypes binding of ``libpygrog_b200.so`` (the C ABI in ``include/pygrog_b200.h``).
+
+There is no fallback: if the library is missing or no CUDA device is
+present, every operation raises.  Tensors are passed as raw device pointers;
+kernels are launched on torch's current CUDA stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import torch
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_lib" / "libpygrog_b200.so"
+
+PGB_C64 = 0
+PGB_C128 = 1
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int
+_f32 = ctypes.c_float
+
+
+class BrickPlanC(ctypes.Structure):
+    """Mirror of ``pgb_brick_plan``."""
+
+    _fields_ = [
+        ("rep_src", _vp),
+        ("rep_meta", _vp),
+        ("rep_w", _vp),
+        ("work", _vp),
+        ("n_work", ctypes.c_int32),
+        ("gz", ctypes.c_int32),
+        ("gy", ctypes.c_int32),
+        ("gx", ctypes.c_int32),
+        ("bz", ctypes.c_int32),
+        ("by", ctypes.c_int32),
+        ("bx", ctypes.c_int32),
+        ("nbz", ctypes.c_int32),
+        ("nby", ctypes.c_int32),
+        ("nbx", ctypes.c_int32),
+        ("split_bricks", _vp),
+        ("n_split_bricks", ctypes.c_int32),
+    ]
+
+
+# name -> argtypes (restype is always c_int status)
+_SIGS = {
+    "pgb_grog_interpolate": [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i32, _vp],
+    "pgb_scatter_add": [_vp, _i64, _vp, _vp, _vp, _i64, _i32, _vp],
+    "pgb_scatter_add_binned": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _i64, _i32, _vp],
+    "pgb_gather": [_vp, _i64, _vp, _vp, _vp, _i64, _i32, _vp],
+    "pgb_psf_scatter_scalar": [_vp, _i64, _vp, _vp, _i64, _i32, _vp],
+    "pgb_psf_scatter_outer": [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _i32, _vp],
+    "pgb_psf_scatter_outer_basis": [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _i32, _vp],
+    "pgb_plan_geometry": [_vp, _i64, _i32, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pgb_plan_gauss_sum": [_vp, _vp, _i64, _vp, _i64, _vp],
+    "pgb_plan_weights": [_vp, _vp, _vp, _i64, _vp, _vp],
+    "pgb_plan_quantize": [_vp, _i64, _i32, _f32, _f32, _f32, _i32, _i64, _vp, _vp],
+    "pgb_grog_grid": [_vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp],
+    "pgb_grog_degrid": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _i32, _vp, _i64, _vp,
+    ],
+    "pgb_grog_expand": [_vp, _i64, _i32, _vp, _vp, _i64, _i64, _i64, _vp, _vp],
+}
+
+_lib = None
+
+
+def exported_names() -> list[str]:
+    """Names of all entry points this binding expects the library to export."""
+    return ["pgb_last_error", "pgb_version", *_SIGS.keys()]
+
+
+def load_library():
+    """Load the shared library (no CUDA device needed to load it)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"pygrog_b200: CUDA library not built ({LIB_PATH}); run "
+            "`python -m pygrog_b200.csrc.build` (there is no CPU fallback)"
+        )
+    lib = ctypes.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL | getattr(os, "RTLD_NOW", 2))
+    lib.pgb_last_error.restype = ctypes.c_char_p
+    lib.pgb_last_error.argtypes = []
+    lib.pgb_version.restype = ctypes.c_char_p
+    lib.pgb_version.argtypes = []
+    for name, argt in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argt
+        fn.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def lib():
+    return load_library()
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        msg = load_library().pgb_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what or 'pygrog_b200'}: {msg or 'error code %d' % status}")
+
+
+def call(name: str, *args) -> None:
+    """Call ``name`` with ``args`` and raise RuntimeError on a non-zero status."""
+    st = getattr(load_library(), name)(*args)
+    check(st, name)
+
+
+def stream_ptr(device=None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def require_cuda(*tensors: torch.Tensor, what: str = "pygrog_b200") -> None:
+    for t in tensors:
+        if t is not None and t.device.type != "cuda":
+            raise RuntimeError(
+                f"{what}: tensors must be on a CUDA device (pygrog_b200 has no CPU path); "
+                f"got device {t.device}"
+            )
+
+
+def dtype_code(t: torch.Tensor, what: str) -> int:
+    if t.dtype in (torch.complex64, torch.float32):
+        return PGB_C64
+    if t.dtype in (torch.complex128, torch.float64):
+        return PGB_C128
+    raise RuntimeError(f"{what}: expected ComplexFloat or ComplexDouble, got {t.dtype}")

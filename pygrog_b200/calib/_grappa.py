@@ -1,0 +1,147 @@
+"""GRAPPA unit-shift operators and the fractional-shift GROG table.
+
+Restates the reference algorithm of ``calib/_grappa.py`` (FiRMLAB-Pisa/pygrog):
+
+* ``lstsq`` (``_grappa.py:16-59``): Tikhonov least squares through the
+  augmented system ``[A; sqrt(lam) I] X = [B; 0]`` solved by LAPACK gelsd;
+* unit operators (``_grappa.py:264-367``): the calibration block is scaled to
+  unit Frobenius norm and, per spatial axis, ``S @ G.T = T`` is solved for
+  neighbour pairs along that axis;
+* fractional powers (``_grappa.py:62-72, 184-208``): ``G^d = expm(d logm G)``
+  with ``logm`` through a complex128 eigendecomposition;
+* the table (``_grappa.py:75-181``): ``nsteps = 2*radius/10^-p + 1`` shifts
+  per axis and ``table[i*n + j] = Gx[j] @ Gy[i]`` (2-D) or
+  ``table[i*n^2 + j*n + k] = Gx[k] @ Gy[j] @ Gz[i]`` (3-D).
+
+The operator naming follows the reference exactly, including its axis
+convention: in 2-D ``Gx`` shifts along spatial axis 0 and ``Gy`` along axis
+1; in 3-D ``Gz`` shifts along axis 0, ``Gy`` along axis 1, ``Gx`` along
+axis 2.  The same library calls (torch.linalg on the host CPU) are used so
+that a table computed here is bit-identical to the reference's on the same
+machine.
+
+The fit is tiny (a few C x C solves) and stays on the host CPU in the
+caller's precision; ``fit_dtype=torch.complex128`` runs the whole fit in
+FP64 and casts only the finished table.
+"""
+
+from __future__ import annotations
+
+__all__ = ["KernelTable", "lstsq", "grappa_power", "prepare_grappa_table", "train_grappa"]
+
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+
+def lstsq(A, b, lamda: float = 0.0):
+    """Tikhonov-regularised least squares ``min ||A X - B||^2 + lamda ||X||^2``."""
+    A_t = torch.as_tensor(A)
+    b_t = torch.as_tensor(b)
+    n = A_t.shape[-1]
+    if lamda > 0:
+        reg = (lamda**0.5) * torch.eye(n, dtype=A_t.dtype, device=A_t.device)
+        if A_t.dim() > 2:
+            reg = reg.expand(*A_t.shape[:-2], n, n)
+        pad = torch.zeros(*A_t.shape[:-2], n, b_t.shape[-1], dtype=b_t.dtype, device=b_t.device)
+        A_t = torch.cat([A_t, reg], dim=-2)
+        b_t = torch.cat([b_t, pad], dim=-2)
+    sol = torch.linalg.lstsq(A_t, b_t, driver="gelsd").solution
+    return sol.numpy() if isinstance(A, np.ndarray) else sol
+
+
+def _logm(A: torch.Tensor) -> torch.Tensor:
+    """Matrix logarithm ``V diag(log lam) V^-1`` evaluated in complex128."""
+    out_dtype = A.dtype if A.is_complex() else torch.complex64
+    vals, vecs = torch.linalg.eig(A.to(torch.complex128))
+    return (vecs @ torch.diag_embed(torch.log(vals)) @ torch.linalg.inv(vecs)).to(out_dtype)
+
+
+def grappa_power(G_unit: torch.Tensor, exponents: torch.Tensor) -> torch.Tensor:
+    """Stack of ``G_unit ** e`` for each exponent, shape ``(len(e), C, C)``."""
+    G_unit = torch.as_tensor(G_unit)
+    e = torch.as_tensor(exponents, dtype=torch.float32)
+    L = _logm(G_unit)
+    return torch.linalg.matrix_exp(e.to(L.dtype).view(-1, 1, 1) * L.unsqueeze(0)).to(G_unit.dtype)
+
+
+def _unit_operators(calib: torch.Tensor, lamda: float) -> list[torch.Tensor]:
+    """Per-axis unit shift operators; entry ``a`` shifts along spatial axis a."""
+    calib = calib / torch.linalg.norm(calib)
+    cal = calib.movedim(0, -1)  # (*spatial, C)
+    nc = cal.shape[-1]
+    ops = []
+    for axis in range(cal.ndim - 1):
+        m = cal.shape[axis] - 1
+        src = cal.narrow(axis, 0, m).reshape(-1, nc)
+        dst = cal.narrow(axis, 1, m).reshape(-1, nc)
+        ops.append(lstsq(src, dst, lamda).mT)
+    return ops
+
+
+def train_grappa(train_data, lamda: float | None = None) -> SimpleNamespace:
+    """Unit GROG operators ``x``, ``y`` (and ``z`` in 3-D) from a Cartesian ACR."""
+    if lamda is None:
+        lamda = 0.01
+    t = torch.as_tensor(train_data)
+    ndim = t.ndim - 1
+    ops = _unit_operators(t, lamda)
+    if ndim == 2:
+        return SimpleNamespace(x=ops[0], y=ops[1], z=None)
+    if ndim == 3:
+        return SimpleNamespace(x=ops[2], y=ops[1], z=ops[0])
+    raise ValueError(f"GROG interpolation only supports 2D or 3D data, got {ndim}D")
+
+
+def prepare_grappa_table(Gx, Gy, Gz, nsteps: int, ndim: int) -> torch.Tensor:  # noqa: ARG001
+    """Product table of per-axis fractional operators (row-major shift index)."""
+    Gx = torch.as_tensor(Gx)
+    Gy = torch.as_tensor(Gy)
+    if ndim == 2:
+        return (Gx[None] @ Gy[:, None]).reshape(-1, *Gx.shape[-2:])
+    if ndim == 3:
+        if Gz is None:
+            raise ValueError("3D interpolation requires Z operator")
+        Gz = torch.as_tensor(Gz)
+        return (Gx[None, None] @ Gy[None, :, None] @ Gz[:, None, None]).reshape(-1, *Gx.shape[-2:])
+    raise ValueError(f"GROG interpolation only supports 2D or 3D data, got {ndim}D")
+
+
+def shift_steps(radius: float, precision: int) -> tuple[float, int, torch.Tensor]:
+    """Quantisation step, number of steps and the float32 shift of each step."""
+    stepsize = 10 ** (-precision)
+    nsteps = int(2 * radius / stepsize + 1)
+    deltas = (torch.arange(nsteps).float() - (nsteps - 1) / 2) * stepsize
+    return stepsize, nsteps, deltas
+
+
+def KernelTable(
+    train_data,
+    radius: float,
+    precision: int = 1,
+    lamda: float = 0.01,
+    fit_dtype: torch.dtype | None = None,
+):
+    """Return ``(table (nsteps**ndim, C, C) ndarray, nsteps, ndim)``.
+
+    ``fit_dtype`` (e.g. ``torch.complex128``) runs the least squares, logm and
+    expm in that precision and casts the table back to the ACR's dtype.
+    """
+    t = torch.as_tensor(np.asarray(train_data)) if isinstance(train_data, np.ndarray) else torch.as_tensor(train_data)
+    t = t.detach().cpu()
+    out_dtype = t.dtype if t.is_complex() else torch.complex64
+    if fit_dtype is not None:
+        t = t.to(fit_dtype)
+    ops = train_grappa(t, lamda)
+    _, nsteps, deltas = shift_steps(radius, precision)
+    Gx = grappa_power(ops.x, deltas)
+    Gy = grappa_power(ops.y, deltas)
+    if ops.z is not None:
+        Gz = grappa_power(ops.z, deltas)
+        ndim = 3
+    else:
+        Gz = None
+        ndim = 2
+    table = prepare_grappa_table(Gx, Gy, Gz, nsteps, ndim).to(out_dtype)
+    return table.numpy(), nsteps, ndim

@@ -1,0 +1,775 @@
+"""GROG interpolator on the GPU: plan, shift table, interpolation and gridding.
+
+Mirrors the public API of ``calib/_grog.py`` (FiRMLAB-Pisa/pygrog):
+``GrogPlan`` (27-181), ``GrogInterpolator(shape, coords, oversamp,
+kernel_width, kernel_shape, time_map, image_shape, stack_shape)`` (302-331),
+``calc_interp_table`` (382-422), ``interpolate`` (437-555), shot-by-shot
+gridding (697-731, 904-912) and ``fft_plan`` (348-376).
+
+What runs where:
+* plan geometry, EGROG weights and shift quantisation: CUDA kernels with
+  bit-exact float32 integer keys (``csrc/plan.cu``); sorting by cell:
+  device radix sort;
+* GRAPPA table fit: host LAPACK, as in the reference (a few C x C solves);
+* ``interpolate``: one replica-expansion kernel (``csrc/grog_fused.cu``)
+  instead of replicate / transpose / matvec / copy-back passes;
+* ``interpolate(grid=True)``: one fused kernel (shift matvec, EGROG weight,
+  scatter) writing every grid cell once;
+* :meth:`GrogInterpolator.degrid`: its exact adjoint (new; the reference has
+  no adjoint of the GROG shift).
+
+Plan fields live on the GPU.  Inputs may be numpy arrays or tensors on any
+device; numpy inputs give numpy outputs like the reference.
+"""
+
+from __future__ import annotations
+
+__all__ = ["GrogInterpolator", "GrogPlan", "BrickPlan"]
+
+import math
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ._grappa import KernelTable
+
+_DEFAULT_DEVICE = "cuda"
+
+
+# ---------------------------------------------------------------------------
+# Plan container
+# ---------------------------------------------------------------------------
+class GrogPlan(SimpleNamespace):
+    """Namespace of GROG / FFT plan fields (reference ``GrogPlan``).
+
+    ``pre_weights`` is computed from ``sqrt_weights`` and ``inv_perm`` so it
+    always matches :meth:`GrogInterpolator.interpolate` output order.
+    """
+
+    @property
+    def stack_shape(self) -> tuple:
+        return tuple(getattr(self, "_stack_shape", ()))
+
+    @stack_shape.setter
+    def stack_shape(self, value):
+        self._stack_shape = tuple(int(s) for s in (value or ()))
+
+    @property
+    def is_stacked(self) -> bool:
+        return len(self.stack_shape) > 0
+
+    @property
+    def pre_weights(self) -> torch.Tensor:
+        sw = self.sqrt_weights
+        ip = self.inv_perm
+        if not self.is_stacked:
+            return sw[ip]
+        return torch.gather(sw, -1, ip)
+
+    @classmethod
+    def _stack(cls, plans: list) -> "GrogPlan":
+        if not plans:
+            raise ValueError("Cannot stack an empty list of plans.")
+        for p in plans:
+            if getattr(p, "stack_shape", ()) != ():
+                raise ValueError("GrogPlan.stack requires unstacked input plans.")
+        ref = plans[0]
+        global_fields = (
+            "shape", "oversamp", "grid_shape", "kernel_width", "kernel_shape", "radius",
+            "image_shape", "grid_size", "n_samples", "natural_shape",
+        )
+        for f in global_fields:
+            v = getattr(ref, f, None)
+            for p in plans[1:]:
+                if getattr(p, f, None) != v:
+                    raise ValueError(f"GrogPlan.stack: field '{f}' differs across plans")
+        out = cls(**{f: getattr(ref, f) for f in global_fields})
+        out.stack_shape = (len(plans),)
+        for f in ("target_idx", "weights", "indices", "sqrt_weights", "sort_perm", "inv_perm"):
+            setattr(out, f, torch.stack([getattr(p, f) for p in plans], dim=0))
+        if all(getattr(p, "distances", None) is not None for p in plans):
+            out.distances = torch.stack([p.distances for p in plans], dim=0)
+        else:
+            out.distances = None
+        if any(p.time_map is not None for p in plans):
+            if any(p.time_map is None for p in plans):
+                raise ValueError("GrogPlan.stack: all plans must agree on time_map presence")
+            out.time_map = torch.stack([p.time_map for p in plans], dim=0)
+        else:
+            out.time_map = None
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Plan helpers (host: tiny integer tables and the coordinate rescale)
+# ---------------------------------------------------------------------------
+def _kernel_offsets(ndim: int, width: int, shape: str) -> np.ndarray:
+    """Integer neighbourhood offsets ``(kw, ndim)`` (reference ``_grog.py:1240-1277``).
+
+    Width ``w`` spans ``arange(w) - floor((w-1)/2)`` per axis; ``circle`` /
+    ``sphere`` keep ``|o| <= (w-1)/2 + 0.5``, ``cross`` keeps offsets with at
+    most one non-zero component, ``square`` / ``cube`` keep all, in C order.
+    """
+    half = (width - 1) / 2.0
+    ax = np.arange(width) - int(np.floor(half))
+    grids = np.meshgrid(*([ax] * ndim), indexing="ij")
+    offs = np.stack([g.ravel() for g in grids], axis=-1).astype(np.int32)
+    key = shape.lower()
+    if key in ("square", "cube"):
+        return offs
+    if key in ("circle", "sphere"):
+        r = np.sqrt((offs.astype(np.float32) ** 2).sum(axis=-1))
+        return offs[r <= half + 0.5]
+    if key == "cross":
+        return offs[(offs != 0).sum(axis=-1) <= 1]
+    raise ValueError(
+        f"Unknown kernel_shape '{shape}'. Use 'circle'/'sphere', 'square'/'cube', or 'cross'."
+    )
+
+
+def _default_shape(ndim, shape):
+    if np.isscalar(shape):
+        shape = ndim * [shape]
+    return tuple(int(s) for s in shape)
+
+
+def _default_oversamp(ndim, oversamp):
+    if oversamp is None:
+        oversamp = (1.0, 1.0) if ndim == 2 else (1.0, 1.0, 1.2)
+    if np.isscalar(oversamp):
+        oversamp = ndim * [oversamp]
+    oversamp = tuple(oversamp)
+    if len(oversamp) != ndim:
+        raise ValueError(f"Oversampling {oversamp} does not match ndim={ndim}")
+    return oversamp
+
+
+def _rescale_coords(coords: np.ndarray, amp) -> np.ndarray:
+    """``0.5 * amp * coords / max|coords|`` per axis, in float32 (``_grog.py:1318-1322``)."""
+    cmax = np.abs(coords).reshape(-1, coords.shape[-1]).max(axis=0)
+    if np.isscalar(amp):
+        amp = coords.shape[-1] * [amp]
+    return 0.5 * np.asarray(amp, dtype=coords.dtype) * coords / cmax
+
+
+def _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, time_map, device):
+    """Per-replica target cells, shifts and EGROG weights on the device.
+
+    Follows ``_create_plan_single`` (``_grog.py:1081-1234``); the arithmetic is
+    in ``pgb_plan_geometry`` / ``pgb_plan_gauss_sum`` / ``pgb_plan_weights``.
+    """
+    coords = np.asarray(coords, dtype=np.float32)
+    ndim = coords.shape[-1]
+    if ndim not in (2, 3):
+        raise ValueError(f"GROG interpolation only supports 2D or 3D data, got {ndim}D")
+    shape = _default_shape(ndim, shape)
+    oversamp = _default_oversamp(ndim, oversamp)
+    grid_shape = tuple(int(np.ceil(s * o)) for s, o in zip(shape, oversamp))
+    amp = [2 * (s - 1 - s // 2) for s in shape]
+    coords_scaled = np.ascontiguousarray(_rescale_coords(coords, amp), dtype=np.float32)
+    offsets = _kernel_offsets(ndim, kernel_width, kernel_shape)
+    kw = int(offsets.shape[0])
+    origins = np.asarray([-(s // 2) for s in shape], dtype=np.float32)
+    steps = np.asarray(
+        [(s - 1) / (gs - 1) if gs > 1 else 1.0 for s, gs in zip(shape, grid_shape)], dtype=np.float32
+    )
+    lead = coords.shape[:-1]
+    npts = int(np.prod(lead)) if lead else 1
+    R = npts * kw
+    G = int(np.prod(grid_shape))
+    dev = torch.device(device)
+    c_d = torch.from_numpy(coords_scaled.reshape(npts, ndim)).to(dev)
+    off_d = torch.from_numpy(np.ascontiguousarray(offsets)).to(dev)
+    gs_d = torch.tensor(grid_shape, dtype=torch.int64, device=dev)
+    org_d = torch.from_numpy(origins).to(dev)
+    stp_d = torch.from_numpy(steps).to(dev)
+    target = torch.empty(R, dtype=torch.int64, device=dev)
+    dist = torch.empty(R, ndim, dtype=torch.float32, device=dev)
+    gauss = torch.empty(R, dtype=torch.float32, device=dev)
+    s = _lib.stream_ptr(dev)
+    _lib.call(
+        "pgb_plan_geometry", c_d.data_ptr(), npts, ndim, off_d.data_ptr(), kw, gs_d.data_ptr(),
+        org_d.data_ptr(), stp_d.data_ptr(), target.data_ptr(), dist.data_ptr(), gauss.data_ptr(), s,
+    )
+    gsum = torch.zeros(G, dtype=torch.float64, device=dev)
+    _lib.call("pgb_plan_gauss_sum", target.data_ptr(), gauss.data_ptr(), R, gsum.data_ptr(), G, s)
+    weights = torch.empty(R, dtype=torch.float32, device=dev)
+    _lib.call(
+        "pgb_plan_weights", target.data_ptr(), gauss.data_ptr(), gsum.data_ptr(), R,
+        weights.data_ptr(), s,
+    )
+    del gsum, gauss
+    if time_map is not None:
+        tm = torch.as_tensor(np.asarray(time_map, dtype=np.float32), device=dev)
+        time_map = tm.reshape(*lead, 1).expand(*lead, kw).contiguous()
+    return GrogPlan(
+        shape=shape,
+        oversamp=oversamp,
+        grid_shape=grid_shape,
+        kernel_width=kernel_width,
+        kernel_shape=kernel_shape,
+        radius=0.5,
+        target_idx=target.reshape(*lead, kw),
+        distances=dist.reshape(*lead, kw, ndim),
+        weights=weights.reshape(*lead, kw),
+        time_map=time_map,
+    )
+
+
+def _attach_fft_plan(plan, image_shape=None):
+    """Sorted-by-cell FFT fields (``_grog.py:918-998``), on the device.
+
+    Invalid replicas keep index 0 and weight 0 so ``n_samples = N * kw``.
+    The sort is stable (the reference's is not; only the order among
+    replicas of the same cell can differ, which no result depends on).
+    """
+    grid_shape = tuple(plan.grid_shape)
+    if image_shape is None:
+        image_shape = tuple(plan.shape)
+    elif np.isscalar(image_shape):
+        image_shape = len(grid_shape) * (int(image_shape),)
+    image_shape = tuple(int(s) for s in image_shape)
+    grid_size = int(np.prod(grid_shape))
+    s_shape = tuple(getattr(plan, "stack_shape", ()) or ())
+    tgt = plan.target_idx
+    natural_shape = tuple(int(s) for s in tgt.shape[len(s_shape):])
+    n_per = int(np.prod(natural_shape)) if natural_shape else 0
+    idx = tgt.reshape(*s_shape, n_per).to(torch.int64).clone()
+    w = plan.weights.reshape(*s_shape, n_per).to(torch.float32)
+    sqrt_w = torch.sqrt(w.clamp(min=0.0))
+    invalid = idx < 0
+    idx = torch.where(invalid, torch.zeros_like(idx), idx)
+    sqrt_w = torch.where(invalid, torch.zeros_like(sqrt_w), sqrt_w)
+    sorted_idx, sort_perm = torch.sort(idx, dim=-1, stable=True)
+    sorted_w = torch.gather(sqrt_w, -1, sort_perm)
+    inv_perm = torch.empty_like(sort_perm)
+    ar = torch.arange(n_per, dtype=torch.int64, device=idx.device).expand(sort_perm.shape)
+    inv_perm.scatter_(-1, sort_perm, ar)
+    plan.image_shape = image_shape
+    plan.grid_size = grid_size
+    plan.n_samples = n_per
+    plan.natural_shape = natural_shape
+    plan.indices = sorted_idx
+    plan.sqrt_weights = sorted_w
+    plan.sort_perm = sort_perm
+    plan.inv_perm = inv_perm
+
+
+def _create_plan(shape, coords, oversamp, kernel_width, kernel_shape, time_map, stack_shape, device):
+    s_shape = tuple(int(s) for s in (stack_shape or ()))
+    if not s_shape:
+        return _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, time_map, device)
+    coords = np.asarray(coords)
+    if tuple(coords.shape[: len(s_shape)]) != s_shape:
+        raise ValueError(
+            f"coords leading shape {coords.shape[: len(s_shape)]} does not match stack_shape {s_shape}"
+        )
+    s_total = int(np.prod(s_shape))
+    cflat = coords.reshape(s_total, *coords.shape[len(s_shape):])
+    if time_map is not None:
+        tm = np.asarray(time_map)
+        if tm.shape[: len(s_shape)] != s_shape:
+            raise ValueError(
+                f"time_map leading shape {tm.shape[: len(s_shape)]} does not match stack_shape {s_shape}"
+            )
+        tflat = tm.reshape(s_total, *tm.shape[len(s_shape):])
+    else:
+        tflat = [None] * s_total
+    plans = [
+        _create_plan_single(shape, cflat[i], oversamp, kernel_width, kernel_shape, tflat[i], device)
+        for i in range(s_total)
+    ]
+    for p in plans:
+        _attach_fft_plan(p, image_shape=None)
+    out = GrogPlan._stack(plans)
+    if len(s_shape) > 1:
+        for f in ("target_idx", "weights", "indices", "sqrt_weights", "sort_perm", "inv_perm"):
+            t = getattr(out, f)
+            setattr(out, f, t.reshape(s_shape + tuple(t.shape[1:])))
+        if out.time_map is not None:
+            out.time_map = out.time_map.reshape(s_shape + tuple(out.time_map.shape[1:]))
+        out.stack_shape = s_shape
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Brick work plan for the fused grid / degrid kernels
+# ---------------------------------------------------------------------------
+def _u32_to_i32(x: torch.Tensor) -> torch.Tensor:
+    return torch.where(x >= 2**31, x - 2**32, x).to(torch.int32)
+
+
+class BrickPlan:
+    """Valid replicas sorted by (brick, cell) with packed per-replica metadata.
+
+    Per replica: ``rep_src`` int32 source sample, ``rep_meta`` uint32 (table
+    entry in the low 20 bits, cell-in-brick above), ``rep_w`` float32 weight.
+    ``work`` rows ``{brick, begin, end, split}`` give each CTA one brick or one
+    chunk of at most ``chunk`` replicas of a hot brick.
+    """
+
+    def __init__(
+        self,
+        target_idx: torch.Tensor,
+        interp_idx: torch.Tensor,
+        rep_weight: torch.Tensor,
+        kw: int,
+        grid_shape,
+        brick=None,
+        chunk: int = 2048,
+    ):
+        dev = target_idx.device
+        grid_shape = tuple(int(s) for s in grid_shape)
+        if len(grid_shape) == 2:
+            gz, gy, gx = 1, grid_shape[0], grid_shape[1]
+            bz, by, bx = brick if brick is not None else (1, 16, 32)
+        else:
+            gz, gy, gx = grid_shape
+            bz, by, bx = brick if brick is not None else (8, 8, 8)
+        bz, by, bx = min(bz, gz), min(by, gy), min(bx, gx)
+        self.grid = (gz, gy, gx)
+        self.brick = (bz, by, bx)
+        self.nb = ((gz + bz - 1) // bz, (gy + by - 1) // by, (gx + bx - 1) // bx)
+        self.cells = bz * by * bx
+        if self.cells > 4096:
+            raise ValueError("brick too large (max 4096 cells)")
+        n_bricks = self.nb[0] * self.nb[1] * self.nb[2]
+        tgt = target_idx.reshape(-1)
+        R = tgt.numel()
+        self.n_src = R // kw
+        valid = tgt >= 0
+        r = torch.nonzero(valid).squeeze(1)
+        t = tgt[r]
+        z = t // (gy * gx)
+        rem = t - z * (gy * gx)
+        y = rem // gx
+        x = rem - y * gx
+        brick_id = ((z // bz) * self.nb[1] + (y // by)) * self.nb[2] + (x // bx)
+        cl = ((z % bz) * by + (y % by)) * bx + (x % bx)
+        key = brick_id * self.cells + cl
+        key_sorted, order = torch.sort(key, stable=True)
+        r = r[order]
+        brick_sorted = key_sorted // self.cells
+        cl_sorted = key_sorted - brick_sorted * self.cells
+        entry = interp_idx.reshape(-1)[r].to(torch.int64)
+        if entry.numel() and int(entry.max()) >= 2**20:
+            raise ValueError("shift table too large for the fused kernels (max 2^20 entries)")
+        self.rep_src = (r // kw).to(torch.int32).contiguous()
+        self.rep_meta = _u32_to_i32(entry | (cl_sorted << 20)).contiguous()
+        self.rep_w = rep_weight.reshape(-1)[r].to(torch.float32).contiguous()
+        self.n_valid = int(r.numel())
+        counts = torch.bincount(brick_sorted, minlength=n_bricks)
+        starts = torch.cumsum(counts, 0) - counts
+        nch = torch.clamp((counts + chunk - 1) // chunk, min=1)
+        bricks_rep = torch.repeat_interleave(torch.arange(n_bricks, device=dev), nch)
+        first = torch.cumsum(nch, 0) - nch
+        k = torch.arange(bricks_rep.numel(), device=dev) - first[bricks_rep]
+        b0 = starts[bricks_rep] + k * chunk
+        b1 = torch.minimum(b0 + chunk, starts[bricks_rep] + counts[bricks_rep])
+        split = (nch[bricks_rep] > 1).to(torch.int64)
+        self.work = torch.stack([bricks_rep, b0, b1, split], dim=1).to(torch.int32).contiguous()
+        nonempty = b1 > b0
+        self.work_nonempty = self.work[nonempty].contiguous()
+        self.split_bricks = torch.nonzero(nch > 1).squeeze(1).to(torch.int32).contiguous()
+        # Samples with no valid replica (zeroed by the adjoint) and whether any
+        # sample has more than one (the adjoint then accumulates atomically).
+        per_src = torch.bincount(self.rep_src.to(torch.int64), minlength=self.n_src)
+        self.multi = bool(int(per_src.max()) > 1) if per_src.numel() else False
+        self.zero_src = torch.nonzero(per_src == 0).squeeze(1).to(torch.int32).contiguous()
+        self._c_all = self._struct(self.work)
+        self._c_nonempty = self._struct(self.work_nonempty)
+
+    def _struct(self, work: torch.Tensor) -> _lib.BrickPlanC:
+        gz, gy, gx = self.grid
+        bz, by, bx = self.brick
+        nbz, nby, nbx = self.nb
+        return _lib.BrickPlanC(
+            self.rep_src.data_ptr(), self.rep_meta.data_ptr(), self.rep_w.data_ptr(),
+            work.data_ptr(), int(work.shape[0]), gz, gy, gx, bz, by, bx, nbz, nby, nbx,
+            self.split_bricks.data_ptr() if self.split_bricks.numel() else None,
+            int(self.split_bricks.numel()),
+        )
+
+    def grid_forward(self, data: torch.Tensor, table: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out (B, C, G) = fused forward of data (B, C, N)``."""
+        B, C, N = data.shape
+        G = out.shape[-1]
+        _lib.call(
+            "pgb_grog_grid", data.data_ptr(), N, out.data_ptr(), G, table.data_ptr(),
+            table.shape[0], C, B, _ctypes_ref(self._c_all), _lib.stream_ptr(data.device),
+        )
+        return out
+
+    def grid_adjoint(self, grid: torch.Tensor, table_h: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out (B, C, N) = adjoint of the fused forward applied to grid (B, C, G)``."""
+        B, C, G = grid.shape
+        N = out.shape[-1]
+        _lib.call(
+            "pgb_grog_degrid", grid.data_ptr(), G, out.data_ptr(), N, table_h.data_ptr(),
+            table_h.shape[0], C, B, _ctypes_ref(self._c_nonempty), 1 if self.multi else 0,
+            self.zero_src.data_ptr() if self.zero_src.numel() else None, int(self.zero_src.numel()),
+            _lib.stream_ptr(grid.device),
+        )
+        return out
+
+
+def _ctypes_ref(s):
+    import ctypes
+
+    return ctypes.byref(s)
+
+
+# ---------------------------------------------------------------------------
+# GrogInterpolator
+# ---------------------------------------------------------------------------
+class GrogInterpolator:
+    """Data-driven GROG interpolator (reference ``GrogInterpolator``).
+
+    Extra keyword ``device`` (default ``"cuda"``) selects the GPU that holds
+    the plan and runs every kernel.
+    """
+
+    _interpolator_set = False
+    _dataset_shape_set = False
+    _data: list | None = None
+
+    def __init__(
+        self,
+        shape,
+        coords,
+        oversamp=None,
+        kernel_width: int = 2,
+        kernel_shape: str = "circle",
+        time_map=None,
+        image_shape=None,
+        stack_shape: tuple = (),
+        *,
+        device=None,
+    ):
+        self.device = torch.device(device if device is not None else _DEFAULT_DEVICE)
+        coords_arr = coords.detach().cpu().numpy() if isinstance(coords, torch.Tensor) else np.asarray(coords)
+        s_eff = tuple(int(s) for s in (stack_shape or ()))
+        if not s_eff and coords_arr.ndim == 4:
+            s_eff = (int(coords_arr.shape[0]),)
+        self.plan = _create_plan(
+            shape, coords_arr, oversamp, kernel_width, kernel_shape, time_map, s_eff, self.device
+        )
+        _attach_fft_plan(self.plan, image_shape)
+        self._brick_plans = None
+        self._density = None
+
+    # -- metadata -----------------------------------------------------------
+    def metadata(self):
+        oshape = np.ceil(np.asarray(self.plan.shape) * np.asarray(self.plan.oversamp)).astype(int).tolist()
+        return SimpleNamespace(
+            shape=tuple(self.plan.shape),
+            oshape=tuple(oshape),
+            target_idx=self.plan.target_idx,
+            weights=self.plan.weights,
+            time_map=self.plan.time_map,
+        )
+
+    def fft_plan(self, image_shape=None):
+        if image_shape is not None and tuple(np.atleast_1d(image_shape)) != tuple(self.plan.image_shape):
+            import copy
+
+            plan = copy.copy(self.plan)
+            _attach_fft_plan(plan, image_shape)
+            return plan
+        return self.plan
+
+    # -- table ----------------------------------------------------------------
+    def calc_interp_table(self, train_data, lamda: float = 0.01, precision: int = 1, *, fit_dtype=None):
+        """Fit the GRAPPA shift table and quantise every replica's shift.
+
+        ``fit_dtype=torch.complex128`` runs the fit in FP64 (table cast back).
+        """
+        if isinstance(train_data, torch.Tensor):
+            train_data = train_data.detach().cpu()
+        table, nsteps, ndim = KernelTable(train_data, self.plan.radius, precision, lamda, fit_dtype)
+        dist = self.plan.distances
+        if dist is None:
+            raise RuntimeError("calc_interp_table: plan distances were already released")
+        K = int(table.shape[0])
+        pfac = 10.0**precision
+        stepsize = 10 ** (-precision)
+        lead = tuple(dist.shape[:-1])
+        R = int(np.prod(lead))
+        idx = torch.empty(lead, dtype=torch.int64, device=self.device)
+        d = dist.contiguous()
+        _lib.call(
+            "pgb_plan_quantize", d.data_ptr(), R, int(dist.shape[-1]), float(self.plan.radius),
+            float(np.float32(pfac)), float(np.float32(stepsize)), int(nsteps), K, idx.data_ptr(),
+            _lib.stream_ptr(self.device),
+        )
+        self.plan.distances = None
+        self._interp_kernel = torch.as_tensor(table)  # host copy (reference field)
+        self._table_d = self._interp_kernel.to(self.device).contiguous()
+        self._table_h_d = self._table_d.conj().transpose(-1, -2).contiguous()
+        self._interp_idx = idx
+        self._interpolator_set = True
+        self._brick_plans = None
+
+    def set_dataset_shape(self, shape):
+        if self._dataset_shape_set:
+            return
+        self.dataset_shape = tuple(shape)
+        self._dataset_shape_set = True
+
+    # -- helpers ----------------------------------------------------------------
+    def _to_device(self, data):
+        is_numpy = isinstance(data, np.ndarray)
+        t = torch.as_tensor(data)
+        src_dev = t.device
+        if not t.is_complex():
+            t = t.to(torch.complex64)
+        return t.to(self.device), is_numpy, src_dev
+
+    def _check_c64(self, t):
+        if t.dtype != torch.complex64:
+            raise RuntimeError(
+                f"GrogInterpolator: the fused GROG kernels compute in complex64, got {t.dtype}"
+            )
+
+    def _split_layout(self, data: torch.Tensor):
+        plan = self.plan
+        s_shape = tuple(plan.stack_shape)
+        s_ndim = len(s_shape)
+        spatial = tuple(int(s) for s in plan.target_idx.shape[s_ndim:-1])
+        kw = int(plan.target_idx.shape[-1])
+        cpos = data.ndim - len(spatial) - 1
+        if cpos < s_ndim:
+            raise ValueError(
+                f"data.ndim={data.ndim} too small for stack_shape={s_shape} + spatial={spatial} (+coils)"
+            )
+        if s_ndim and tuple(int(s) for s in data.shape[cpos - s_ndim : cpos]) != s_shape:
+            raise ValueError(
+                f"data stack prefix {tuple(data.shape[cpos - s_ndim:cpos])} != plan.stack_shape {s_shape}"
+            )
+        if tuple(int(s) for s in data.shape[cpos + 1 :]) != spatial:
+            raise ValueError(f"data spatial dims {tuple(data.shape[cpos + 1:])} != plan {spatial}")
+        batch = tuple(int(s) for s in data.shape[: cpos - s_ndim])
+        return batch, s_shape, int(data.shape[cpos]), spatial, kw
+
+    def _brick(self, s: int) -> BrickPlan:
+        if self._brick_plans is None:
+            self._brick_plans = {}
+        bp = self._brick_plans.get(s)
+        if bp is None:
+            plan = self.plan
+            s_total = int(np.prod(plan.stack_shape)) if plan.stack_shape else 1
+            kw = int(plan.target_idx.shape[-1])
+            tgt = plan.target_idx.reshape(s_total, -1)[s]
+            w = plan.weights.reshape(s_total, -1)[s].clamp(min=0.0)
+            sw = torch.sqrt(w)
+            rep_w = sw * sw
+            idx = self._interp_idx.reshape(s_total, -1)[s]
+            bp = BrickPlan(tgt, idx, rep_w, kw, plan.grid_shape)
+            self._brick_plans[s] = bp
+        return bp
+
+    # -- forward interpolation ------------------------------------------------
+    def interpolate(self, data, shot_index=None, ret_image: bool = False, grid: bool = False):
+        """GROG-shifted replicas ``(*batch, *stack, C, n_samples)`` (see reference)."""
+        if not self._interpolator_set:
+            raise RuntimeError("GRAPPA kernels not set. Call calc_interp_table() first.")
+        if grid and ret_image:
+            raise ValueError("'grid' and 'ret_image' are mutually exclusive.")
+        t, is_numpy, src_dev = self._to_device(data)
+        if shot_index is not None:
+            if np.isscalar(shot_index):
+                shot_index = (shot_index,)
+            g = self._grid_shot(t, tuple(shot_index))
+            if self._data is None:
+                self._data = []
+            self._data.append(g)
+            return None
+        if grid:
+            kgrid, mplan = self._grid_kspace(t)
+            if is_numpy:
+                from ..operator._masked_fft import MaskedFFTPlan
+
+                npplan = MaskedFFTPlan(
+                    grid_shape=mplan.grid_shape, image_shape=mplan.image_shape,
+                    stack_shape=mplan.stack_shape, mask=mplan.mask.cpu().numpy(),
+                    density=mplan.density.cpu().numpy(),
+                )
+                return kgrid.cpu().numpy(), npplan
+            return kgrid.to(src_dev), mplan
+        sparse = self._sparse_flat(t)
+        if ret_image:
+            from ..operator._sparse_fft import SparseFFT
+
+            plan = self.plan
+            op = SparseFFT(plan=plan)
+            pre_w = plan.pre_weights.to(sparse.dtype)
+            pw = pre_w.unsqueeze(-2) if pre_w.ndim > 1 else pre_w.unsqueeze(0)
+            img = op.adjoint(sparse * pw)
+            ax = img.ndim - len(plan.image_shape) - 1
+            image = img.abs().square().sum(ax).sqrt()
+            return image.cpu().numpy() if is_numpy else image.to(src_dev)
+        return sparse.cpu().numpy() if is_numpy else sparse.to(src_dev)
+
+    def __call__(self, data, shot_index=None, ret_image=False, grid=False):
+        return self.interpolate(data, shot_index, ret_image, grid)
+
+    def _sparse_flat(self, data: torch.Tensor) -> torch.Tensor:
+        """Replica expansion, returned as ``(*batch, *stack, C, n_samples)``."""
+        self._check_c64(data)
+        batch, s_shape, C, spatial, kw = self._split_layout(data)
+        B = int(np.prod(batch)) if batch else 1
+        S = int(np.prod(s_shape)) if s_shape else 1
+        N = int(np.prod(spatial))
+        d = data.reshape(B, S, C, N)
+        out = torch.empty(B, S, C, N * kw, dtype=data.dtype, device=data.device)
+        idx = self._interp_idx.reshape(S, N * kw)
+        st = _lib.stream_ptr(data.device)
+        for s in range(S):
+            ds = d[:, s].contiguous() if S > 1 else d.reshape(B, C, N).contiguous()
+            os_ = torch.empty(B, C, N * kw, dtype=data.dtype, device=data.device) if S > 1 else out.view(B, C, N * kw)
+            _lib.call(
+                "pgb_grog_expand", ds.data_ptr(), N, kw, idx[s].contiguous().data_ptr(),
+                self._table_d.data_ptr(), self._table_d.shape[0], C, B, os_.data_ptr(), st,
+            )
+            if S > 1:
+                out[:, s] = os_
+        return out.reshape(*batch, *s_shape, C, N * kw)
+
+    # -- gridded output (fused kernel) ------------------------------------------
+    def _density_grid(self) -> torch.Tensor:
+        """Sum of squared sorted sqrt-weights per cell, ``(*stack, *grid_shape)``."""
+        if self._density is None:
+            plan = self.plan
+            S = int(np.prod(plan.stack_shape)) if plan.stack_shape else 1
+            G = int(plan.grid_size)
+            dens = torch.zeros(S, G, dtype=torch.float32, device=self.device)
+            idx = plan.indices.reshape(S, -1)
+            sw = plan.sqrt_weights.reshape(S, -1)
+            from .. import _ext
+
+            for s in range(S):
+                w_sq = (sw[s] * sw[s]).contiguous()
+                _ext.psf_scatter_scalar(dens[s], idx[s].contiguous(), w_sq)
+            self._density = dens.reshape(*plan.stack_shape, *plan.grid_shape)
+        return self._density
+
+    def _grid_kspace(self, data: torch.Tensor):
+        from ..operator._masked_fft import MaskedFFTPlan
+
+        self._check_c64(data)
+        plan = self.plan
+        batch, s_shape, C, spatial, kw = self._split_layout(data)
+        B = int(np.prod(batch)) if batch else 1
+        S = int(np.prod(s_shape)) if s_shape else 1
+        N = int(np.prod(spatial))
+        G = int(plan.grid_size)
+        d = data.reshape(B, S, C, N)
+        out = torch.empty(B, S, C, G, dtype=data.dtype, device=data.device)
+        for s in range(S):
+            bp = self._brick(s)
+            ds = d[:, s].contiguous()
+            o = torch.empty(B, C, G, dtype=data.dtype, device=data.device) if S > 1 else out.view(B, C, G)
+            bp.grid_forward(ds, self._table_d, o)
+            if S > 1:
+                out[:, s] = o
+        density = self._density_grid()
+        mask = (density > 0).float()
+        kgrid = out.reshape(*batch, *s_shape, C, *plan.grid_shape)
+        mplan = MaskedFFTPlan(
+            grid_shape=tuple(plan.grid_shape), image_shape=tuple(plan.image_shape),
+            stack_shape=tuple(s_shape), mask=mask, density=density,
+        )
+        return kgrid, mplan
+
+    def grid(self, data) -> torch.Tensor:
+        """Fused gridding only: ``interpolate(data, grid=True)[0]`` without the plan object."""
+        if not self._interpolator_set:
+            raise RuntimeError("GRAPPA kernels not set. Call calc_interp_table() first.")
+        t, is_numpy, src_dev = self._to_device(data)
+        self._check_c64(t)
+        plan = self.plan
+        batch, s_shape, C, spatial, kw = self._split_layout(t)
+        B = int(np.prod(batch)) if batch else 1
+        S = int(np.prod(s_shape)) if s_shape else 1
+        N = int(np.prod(spatial))
+        G = int(plan.grid_size)
+        d = t.reshape(B, S, C, N)
+        out = torch.empty(B, S, C, G, dtype=t.dtype, device=t.device)
+        for s in range(S):
+            ds = d[:, s].contiguous()
+            o = torch.empty(B, C, G, dtype=t.dtype, device=t.device) if S > 1 else out.view(B, C, G)
+            self._brick(s).grid_forward(ds, self._table_d, o)
+            if S > 1:
+                out[:, s] = o
+        res = out.reshape(*batch, *s_shape, C, *plan.grid_shape)
+        return res.cpu().numpy() if is_numpy else res.to(src_dev)
+
+    def degrid(self, kgrid):
+        """Adjoint of :meth:`grid` / ``interpolate(grid=True)`` with respect to ``data``.
+
+        ``kgrid (*batch, *stack, C, *grid_shape)`` -> ``(*batch, *stack, C, *spatial)``:
+        ``x[n] = sum_{valid replicas r of n} w_r * T[e_r]^H @ kgrid[cell_r]``.
+        """
+        if not self._interpolator_set:
+            raise RuntimeError("GRAPPA kernels not set. Call calc_interp_table() first.")
+        t, is_numpy, src_dev = self._to_device(kgrid)
+        self._check_c64(t)
+        plan = self.plan
+        s_shape = tuple(plan.stack_shape)
+        gnd = len(plan.grid_shape)
+        if tuple(t.shape[-gnd:]) != tuple(plan.grid_shape):
+            raise ValueError(f"kgrid trailing dims {tuple(t.shape[-gnd:])} != grid_shape {plan.grid_shape}")
+        C = int(t.shape[-gnd - 1])
+        lead = tuple(int(s) for s in t.shape[: t.ndim - gnd - 1])
+        if s_shape and tuple(lead[len(lead) - len(s_shape):]) != s_shape:
+            raise ValueError(f"kgrid stack prefix {lead} must end with {s_shape}")
+        batch = lead[: len(lead) - len(s_shape)]
+        B = int(np.prod(batch)) if batch else 1
+        S = int(np.prod(s_shape)) if s_shape else 1
+        spatial = tuple(int(s) for s in plan.target_idx.shape[len(s_shape):-1])
+        N = int(np.prod(spatial))
+        G = int(plan.grid_size)
+        g = t.reshape(B, S, C, G)
+        out = torch.empty(B, S, C, N, dtype=t.dtype, device=t.device)
+        for s in range(S):
+            gs = g[:, s].contiguous()
+            o = torch.empty(B, C, N, dtype=t.dtype, device=t.device) if S > 1 else out.view(B, C, N)
+            self._brick(s).grid_adjoint(gs, self._table_h_d, o)
+            if S > 1:
+                out[:, s] = o
+        res = out.reshape(*batch, *s_shape, C, *spatial)
+        return res.cpu().numpy() if is_numpy else res.to(src_dev)
+
+    # -- shot-by-shot ---------------------------------------------------------------
+    def _grid_shot(self, data: torch.Tensor, shot_index: tuple) -> torch.Tensor:
+        """Grid one shot ``(C, npts)`` with the plan weights (reference ``_grid_shot``)."""
+        from .. import _ext
+
+        plan = self.plan
+        tgt = plan.target_idx[shot_index].reshape(-1)
+        w = plan.weights[shot_index].reshape(-1).to(torch.float32)
+        idx = self._interp_idx[shot_index].reshape(-1)
+        C = int(data.shape[0])
+        npts = int(data.shape[-1])
+        kw = int(plan.target_idx.shape[-1])
+        self._check_c64(data)
+        rep = data.reshape(C, npts, 1).expand(C, npts, kw).reshape(C, npts * kw)
+        x = rep.transpose(0, 1).reshape(npts * kw, 1, C).contiguous()
+        y = _ext.grog_interpolate(x, idx.contiguous(), self._table_d)[:, 0, :]  # (npts*kw, C)
+        valid = tgt >= 0
+        G = int(np.prod(plan.grid_shape))
+        out = torch.zeros(C, G, dtype=data.dtype, device=data.device)
+        cells = torch.where(valid, tgt, torch.zeros_like(tgt)).contiguous()
+        wv = torch.where(valid, w, torch.zeros_like(w)).contiguous()
+        for c in range(C):
+            _ext.scatter_add(out[c], y[:, c].contiguous(), cells, wv)
+        return out
+
+    def collect_shots(self) -> torch.Tensor:
+        if self._data is None or len(self._data) == 0:
+            raise RuntimeError("No shots accumulated.")
+        out = torch.stack(self._data, dim=0).sum(dim=0)
+        self._data = None
+        return out.reshape(out.shape[0], *self.plan.grid_shape)

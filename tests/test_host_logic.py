@@ -1,0 +1,97 @@
+"""Host-side logic that needs no GPU: brick work plan, offsets, table fit."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, golden_plan_cases, parse_meta, rel_l2
+from oracle import grog as og
+from pygrog_b200.calib import _grog, _grappa
+
+
+@pytest.mark.parametrize("ndim,width,shape", [(2, 2, "circle"), (2, 5, "square"), (3, 2, "sphere"),
+                                             (3, 3, "cube"), (2, 3, "cross"), (3, 4, "cross")])
+def test_kernel_offsets_match_oracle(ndim, width, shape):
+    np.testing.assert_array_equal(_grog._kernel_offsets(ndim, width, shape), og.kernel_offsets(ndim, width, shape))
+
+
+@pytest.mark.parametrize("case", golden_plan_cases())
+def test_table_fit_matches_reference(case):
+    """Host LAPACK table fit == the reference's table (same library calls)."""
+    z = golden(case)
+    name, shape, osf, kwd, ks, prec, C = parse_meta(z["meta"])
+    tab, n, nd = _grappa.KernelTable(z["in_calib"], 0.5, prec, 0.01)
+    assert tab.shape == tuple(z["ref_table_size"])
+    # same LAPACK calls; BLAS thread count changes the last bits (FP32 bar 1e-5)
+    assert rel_l2(tab[z["ref_table_used_idx"]], z["ref_table_used"]) < 1e-5
+
+
+def test_table_fit_fp64_mode_is_close_to_fp32_fit():
+    z = golden("plan_p2d_circle_osf2.npz")
+    t32, _, _ = _grappa.KernelTable(z["in_calib"], 0.5, 1, 0.01)
+    t64, _, _ = _grappa.KernelTable(z["in_calib"], 0.5, 1, 0.01, fit_dtype=torch.complex128)
+    assert t64.dtype == np.complex64
+    assert rel_l2(t32, t64) < 1e-4
+
+
+def _toy_plan(shape, npts, kw, rng, hot=0):
+    G = int(np.prod(shape))
+    tgt = rng.integers(-1, G, size=(npts, kw)).astype(np.int64)
+    if hot:
+        tgt[:hot, 0] = G // 2
+    idx = rng.integers(0, 121, size=(npts, kw)).astype(np.int64)
+    w = rng.random((npts, kw)).astype(np.float32)
+    return torch.from_numpy(tgt), torch.from_numpy(idx), torch.from_numpy(w)
+
+
+@pytest.mark.parametrize("shape", [(40, 70), (20, 17, 33)])
+def test_brick_plan_covers_every_valid_replica_once(shape):
+    rng = np.random.default_rng(1)
+    tgt, idx, w = _toy_plan(shape, 3000, 3, rng, hot=2500)
+    bp = _grog.BrickPlan(tgt, idx, w, 3, shape, chunk=256)
+    work = bp.work.numpy()
+    valid = (tgt.numpy().reshape(-1) >= 0).sum()
+    assert bp.n_valid == valid
+    # chunks tile [0, n_valid) exactly, in order
+    spans = work[:, 1:3]
+    nonempty = spans[spans[:, 1] > spans[:, 0]]
+    assert nonempty[0, 0] == 0 and nonempty[-1, 1] == valid
+    assert np.all(nonempty[1:, 0] == nonempty[:-1, 1])
+    assert np.all(spans[:, 1] - spans[:, 0] <= 256)
+    # every brick appears, hot bricks are split and flagged
+    nb = int(np.prod(bp.nb))
+    assert set(work[:, 0].tolist()) == set(range(nb))
+    assert bp.split_bricks.numel() >= 1 and np.all(work[work[:, 3] == 1, 0] >= 0)
+    # metadata decodes back to the replica's cell, entry and source
+    meta = bp.rep_meta.numpy().astype(np.int64) & 0xFFFFFFFF
+    entry = meta & 0xFFFFF
+    cl = meta >> 20
+    r_sorted = np.nonzero(tgt.numpy().reshape(-1) >= 0)[0]
+    gz, gy, gx = bp.grid
+    bz, by, bx = bp.brick
+    src = bp.rep_src.numpy()
+    # rebuild (brick, cell) from metadata and compare with the true target cell
+    for i in range(0, bp.n_valid, 97):
+        b = int(np.searchsorted(np.cumsum(np.bincount(work[:, 0], minlength=nb) * 0) , 0))
+        del b
+    brick_of = np.empty(bp.n_valid, dtype=np.int64)
+    for row in work:
+        brick_of[row[1]:row[2]] = row[0]
+    nby, nbx = bp.nb[1], bp.nb[2]
+    biz = brick_of // (nby * nbx)
+    biy = (brick_of // nbx) % nby
+    bix = brick_of % nbx
+    lz = cl // (by * bx)
+    ly = (cl // bx) % by
+    lx = cl % bx
+    cell = ((biz * bz + lz) * gy + (biy * by + ly)) * gx + (bix * bx + lx)
+    t_all = tgt.numpy().reshape(-1)
+    i_all = idx.numpy().reshape(-1)
+    # the multiset of (source, cell, entry) triples is preserved
+    got = sorted(zip(src.tolist(), cell.tolist(), entry.tolist()))
+    exp = sorted(zip((r_sorted // 3).tolist(), t_all[r_sorted].tolist(), i_all[r_sorted].tolist()))
+    assert got == exp
+    # sorted by (brick, cell)
+    key = brick_of * bp.cells + cl
+    assert np.all(np.diff(key) >= 0)
+    assert bp.multi == bool(np.bincount(r_sorted // 3).max() > 1)

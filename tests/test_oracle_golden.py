@@ -1,0 +1,85 @@
+"""The oracle (numpy restatement) against golden fixtures from the reference itself.
+
+Integer keys (target cells, shift indices, sorted cell indices) bit-exact;
+distances bit-exact (float32 chain); floats within 1e-5 relative L2.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden, golden_plan_cases, parse_meta, rel_l2
+from oracle import grog as og
+
+
+@pytest.mark.parametrize("case", golden_plan_cases())
+def test_oracle_plan_matches_reference(case):
+    z = golden(case)
+    name, shape, osf, kwd, ks, prec, C = parse_meta(z["meta"])
+    p = og.create_plan(shape, z["in_coords"], osf, kwd, ks)
+    assert tuple(p["grid_shape"]) == tuple(z["ref_grid_shape"])
+    np.testing.assert_array_equal(p["target_idx"], z["ref_target_idx"])
+    np.testing.assert_array_equal(p["distances"], z["ref_distances"])
+    np.testing.assert_allclose(p["weights"], z["ref_weights"], rtol=1e-6, atol=1e-7)
+    fp = og.fft_plan(p)
+    np.testing.assert_array_equal(fp["indices"], z["ref_indices"])
+    # sqrt weights: same multiset per cell (sort ties may be ordered differently)
+    np.testing.assert_allclose(np.sort(fp["sqrt_weights"]), np.sort(z["ref_sqrt_weights"]), rtol=1e-6, atol=1e-7)
+    K = int(z["ref_table_size"][0])
+    nsteps = int(round(K ** (1.0 / len(shape))))
+    qi = og.quantize(p["distances"], prec, nsteps, K)
+    np.testing.assert_array_equal(qi, z["ref_interp_idx"])
+
+
+@pytest.mark.parametrize("case", golden_plan_cases())
+def test_oracle_table_and_grid_match_reference(case):
+    z = golden(case)
+    name, shape, osf, kwd, ks, prec, C = parse_meta(z["meta"])
+    tab, n, nd = og.kernel_table(z["in_calib"], 0.5, prec, 0.01)
+    used = z["ref_table_used_idx"]
+    assert tab.shape == tuple(z["ref_table_size"])
+    assert rel_l2(tab[used], z["ref_table_used"]) < 1e-5
+    # interpolation / gridding with the reference's own table entries
+    full = np.zeros(tuple(z["ref_table_size"]), dtype=np.complex64)
+    full[used] = z["ref_table_used"]
+    p = og.create_plan(shape, z["in_coords"], osf, kwd, ks)
+    data = z["in_data"].reshape(1, C, -1)
+    rep = og.interpolate(data, z["ref_interp_idx"], full)[0]
+    assert rel_l2(rep, z["ref_interpolate"]) < 1e-6
+    kg, dens = og.grid(data, z["ref_interp_idx"], full, p, og.fft_plan(p))
+    assert rel_l2(kg[0], z["ref_kgrid"].reshape(C, -1)) < 1e-5
+    np.testing.assert_allclose(dens, z["ref_density"].reshape(-1), rtol=1e-5, atol=1e-6)
+
+
+def test_oracle_degrid_is_adjoint_of_grid():
+    z = golden("plan_p2d_circle_osf2.npz")
+    name, shape, osf, kwd, ks, prec, C = parse_meta(z["meta"])
+    full = np.zeros(tuple(z["ref_table_size"]), dtype=np.complex64)
+    full[z["ref_table_used_idx"]] = z["ref_table_used"]
+    p = og.create_plan(shape, z["in_coords"], osf, kwd, ks)
+    rng = np.random.default_rng(3)
+    N = z["in_coords"].size // 2
+    G = int(np.prod(p["grid_shape"]))
+    x = (rng.standard_normal((1, C, N)) + 1j * rng.standard_normal((1, C, N))).astype(np.complex128)
+    y = (rng.standard_normal((1, C, G)) + 1j * rng.standard_normal((1, C, G))).astype(np.complex128)
+    fx, _ = og.grid(x, z["ref_interp_idx"], full.astype(np.complex128), p, og.fft_plan(p))
+    ahy = og.degrid(y, z["ref_interp_idx"], full.astype(np.complex128), p)
+    lhs = np.vdot(y.ravel(), fx.ravel())
+    rhs = np.vdot(ahy.ravel(), x.ravel())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-10
+
+
+def test_oracle_l0_primitives_match_reference():
+    z = golden("l0_ops.npz")
+    ref = np.einsum("nij,nbj->nbi", z["gi_kernel"][z["gi_idx"]], z["gi_data"])
+    assert rel_l2(ref, z["ref_gi"]) < 1e-6
+    sa = og.scatter_add(z["sa_grid0"], z["sa_data"], z["sa_idx"], z["sa_w"])
+    assert rel_l2(sa, z["ref_sa"]) < 1e-6
+    ga = og.gather(z["ga_grid"], z["sa_idx"], z["sa_w"])
+    assert rel_l2(ga, z["ref_ga"]) < 1e-7
+    G = z["ref_ps"].size
+    ps = og.psf_scalar(G, z["sa_idx"], z["ps_wsq"])
+    np.testing.assert_allclose(ps, z["ref_ps"], rtol=1e-6, atol=1e-6)
+    po = og.psf_outer(G, z["po_basis"].shape[1], z["sa_idx"], z["ps_wsq"], z["po_basis"])
+    assert rel_l2(po, z["ref_po"]) < 1e-6
+    pb = og.psf_outer_basis(G, z["pb_basis"].shape[0], z["sa_idx"], z["ps_wsq"], z["pb_basis"], z["pb_tix"])
+    assert rel_l2(pb, z["ref_pb"]) < 1e-6
