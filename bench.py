@@ -255,6 +255,7 @@ def run_reference_arm(args):
 
 
 def main():
+    global N_SPOKES, N_READOUT, GRID_N
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -262,7 +263,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--table-mode", default=None, choices=["v5", "v3", "smem", "factored", "global"])
+    ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
+    ap.add_argument("--readout", type=int, default=N_READOUT)
+    ap.add_argument("--grid", type=int, default=GRID_N)
     args = ap.parse_args()
+    resized = (args.spokes, args.readout, args.grid) != (N_SPOKES, N_READOUT, GRID_N)
+    N_SPOKES, N_READOUT, GRID_N = args.spokes, args.readout, args.grid
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":
@@ -283,6 +290,8 @@ def main():
     torch.cuda.set_device(dev)
 
     g, coords, acr, data = build_workload(dev)
+    if args.table_mode:
+        g.gridder_mode = args.table_mode
     bp = g._brick(0)
     G = int(np.prod(g.plan.grid_shape))
     B, C, N = data.shape
@@ -293,10 +302,10 @@ def main():
     def step(evs=None):
         if evs is not None:
             evs[0].record(stream)
-        bp.grid_forward(data, g._table_d, kgrid)
+        bp.forward(data, kgrid)
         if evs is not None:
             evs[1].record(stream)
-        bp.grid_adjoint(kgrid, g._table_h_d, out)
+        bp.adjoint(kgrid, out)
         if evs is not None:
             evs[2].record(stream)
 
@@ -333,12 +342,13 @@ def main():
 
     # algorithmic bytes per launch (both directions): samples + per-replica metadata + grid
     alg_bytes = N * C * 8 * B + bp.n_valid * 12 + G * C * 8 * B
-    dom = "grog_grid_kernel" if fwd_ms >= adj_ms else "grog_degrid_kernel"
+    kname = {"v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(bp.mode, "factored_kernel")
+    dom = f"grog_grid_{kname}" if fwd_ms >= adj_ms else f"grog_degrid_{kname}"
     dom_ms = max(fwd_ms, adj_ms)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     traffic, tsrc = _profile_traffic(dom)
-    n_launch = (2 if bp.split_bricks.numel() else 1) + (1 if (not bp.multi and bp.zero_src.numel()) else 0) + 1
+    n_launch = bp.launches_per_call(False) + bp.launches_per_call(True)
 
     # end to end through the public API with host buffers (pinned)
     e2e = None
@@ -386,10 +396,11 @@ def main():
             "dtype": "c64",
             "data": "synthetic",
             "config": {
-                "workload": "grog3d_kooshball_192c12_fwd_adj",
+                "workload": (f"grog3d_kooshball_{GRID_N}c12_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
+                             else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
             "fwd_ms": fwd_ms,

@@ -66,6 +66,32 @@ _SIGS = {
         _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _i32, _vp, _i64, _vp,
     ],
     "pgb_grog_expand": [_vp, _i64, _i32, _vp, _vp, _i64, _i64, _i64, _vp, _vp],
+    "pgb_grog_grid_factored": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
+    ],
+    "pgb_grog_degrid_factored": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _i32,
+        _vp, _i64, _vp,
+    ],
+    "pgb_grog_grid_v3": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
+    ],
+    "pgb_grog_degrid_v3": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC),
+        ctypes.POINTER(BrickPlanC), _vp, _i64, _vp,
+    ],
+    "pgb_grog_grid_v5": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
+    ],
+    "pgb_grog_degrid_v5": [
+        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC),
+        ctypes.POINTER(BrickPlanC), _vp, _i64, _vp,
+    ],
+}
+_SIZE_FUNCS = {
+    "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],
+    "pgb_grog_v3_smem_bytes": [_i64, _i64, _i64, _i32],
+    "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
 }
 
 _lib = None
@@ -73,7 +99,7 @@ _lib = None
 
 def exported_names() -> list[str]:
     """Names of all entry points this binding expects the library to export."""
-    return ["pgb_last_error", "pgb_version", *_SIGS.keys()]
+    return ["pgb_last_error", "pgb_version", *_SIGS.keys(), *_SIZE_FUNCS.keys()]
 
 
 def load_library():
@@ -95,6 +121,10 @@ def load_library():
         fn = getattr(lib, name)
         fn.argtypes = argt
         fn.restype = ctypes.c_int
+    for name, argt in _SIZE_FUNCS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argt
+        fn.restype = ctypes.c_size_t
     _lib = lib
     return lib
 

@@ -27,7 +27,7 @@ FP64 and casts only the finished table.
 
 from __future__ import annotations
 
-__all__ = ["KernelTable", "lstsq", "grappa_power", "prepare_grappa_table", "train_grappa"]
+__all__ = ["KernelTable", "lstsq", "grappa_power", "prepare_grappa_table", "table_factors", "train_grappa"]
 
 from types import SimpleNamespace
 
@@ -116,17 +116,39 @@ def shift_steps(radius: float, precision: int) -> tuple[float, int, torch.Tensor
     return stepsize, nsteps, deltas
 
 
+def table_factors(Gx, Gy, Gz, ndim: int):
+    """Split the table as ``T[e] = outer[e % n] @ inner[e // n]``.
+
+    2-D: ``T[i*n + j] = Gx[j] @ Gy[i]``          -> outer = Gx, inner = Gy.
+    3-D: ``T[i*n^2 + j*n + k] = Gx[k] @ Gy[j] @ Gz[i]``
+                                                   -> outer = Gx,
+                                                      inner[i*n + j] = Gy[j] @ Gz[i].
+    The fused kernels keep ``inner`` in shared memory and apply ``outer`` once
+    per run of replicas that share its index and target cell.
+    """
+    Gx = torch.as_tensor(Gx)
+    Gy = torch.as_tensor(Gy)
+    if ndim == 2:
+        return Gx.contiguous(), Gy.contiguous()
+    Gz = torch.as_tensor(Gz)
+    inner = (Gy[None, :] @ Gz[:, None]).reshape(-1, *Gx.shape[-2:])
+    return Gx.contiguous(), inner.contiguous()
+
+
 def KernelTable(
     train_data,
     radius: float,
     precision: int = 1,
     lamda: float = 0.01,
     fit_dtype: torch.dtype | None = None,
+    return_factors: bool = False,
 ):
     """Return ``(table (nsteps**ndim, C, C) ndarray, nsteps, ndim)``.
 
     ``fit_dtype`` (e.g. ``torch.complex128``) runs the least squares, logm and
     expm in that precision and casts the table back to the ACR's dtype.
+    With ``return_factors`` a fourth item ``(outer, inner)`` is returned (see
+    :func:`table_factors`), cast like the table.
     """
     t = torch.as_tensor(np.asarray(train_data)) if isinstance(train_data, np.ndarray) else torch.as_tensor(train_data)
     t = t.detach().cpu()
@@ -144,4 +166,7 @@ def KernelTable(
         Gz = None
         ndim = 2
     table = prepare_grappa_table(Gx, Gy, Gz, nsteps, ndim).to(out_dtype)
+    if return_factors:
+        outer, inner = table_factors(Gx, Gy, Gz, ndim)
+        return table.numpy(), nsteps, ndim, (outer.to(out_dtype), inner.to(out_dtype))
     return table.numpy(), nsteps, ndim

@@ -24,7 +24,7 @@ device; numpy inputs give numpy outputs like the reference.
 
 from __future__ import annotations
 
-__all__ = ["GrogInterpolator", "GrogPlan", "BrickPlan"]
+__all__ = ["GrogInterpolator", "GrogPlan", "BrickPlan", "GrogGridder"]
 
 import math
 from types import SimpleNamespace
@@ -182,16 +182,17 @@ def _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, tim
     dev = torch.device(device)
     c_d = torch.from_numpy(coords_scaled.reshape(npts, ndim)).to(dev)
     off_d = torch.from_numpy(np.ascontiguousarray(offsets)).to(dev)
-    gs_d = torch.tensor(grid_shape, dtype=torch.int64, device=dev)
-    org_d = torch.from_numpy(origins).to(dev)
-    stp_d = torch.from_numpy(steps).to(dev)
+    # per-axis parameters are read by the host launcher: pass host arrays
+    gs_h = np.ascontiguousarray(grid_shape, dtype=np.int64)
+    org_h = np.ascontiguousarray(origins, dtype=np.float32)
+    stp_h = np.ascontiguousarray(steps, dtype=np.float32)
     target = torch.empty(R, dtype=torch.int64, device=dev)
     dist = torch.empty(R, ndim, dtype=torch.float32, device=dev)
     gauss = torch.empty(R, dtype=torch.float32, device=dev)
     s = _lib.stream_ptr(dev)
     _lib.call(
-        "pgb_plan_geometry", c_d.data_ptr(), npts, ndim, off_d.data_ptr(), kw, gs_d.data_ptr(),
-        org_d.data_ptr(), stp_d.data_ptr(), target.data_ptr(), dist.data_ptr(), gauss.data_ptr(), s,
+        "pgb_plan_geometry", c_d.data_ptr(), npts, ndim, off_d.data_ptr(), kw, gs_h.ctypes.data,
+        org_h.ctypes.data, stp_h.ctypes.data, target.data_ptr(), dist.data_ptr(), gauss.data_ptr(), s,
     )
     gsum = torch.zeros(G, dtype=torch.float64, device=dev)
     _lib.call("pgb_plan_gauss_sum", target.data_ptr(), gauss.data_ptr(), R, gsum.data_ptr(), G, s)
@@ -319,16 +320,21 @@ class BrickPlan:
         grid_shape,
         brick=None,
         chunk: int = 2048,
+        n_outer: int = 1,
+        pack: str = "wide",
+        mask: torch.Tensor | None = None,
+        order: str = "cell",
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
+        self.n_outer = int(n_outer)
         if len(grid_shape) == 2:
             gz, gy, gx = 1, grid_shape[0], grid_shape[1]
             bz, by, bx = brick if brick is not None else (1, 16, 32)
         else:
             gz, gy, gx = grid_shape
             bz, by, bx = brick if brick is not None else (8, 8, 8)
-        bz, by, bx = min(bz, gz), min(by, gy), min(bx, gx)
+        # partial bricks at the grid edge are bounds-checked by the kernels
         self.grid = (gz, gy, gx)
         self.brick = (bz, by, bx)
         self.nb = ((gz + bz - 1) // bz, (gy + by - 1) // by, (gx + bx - 1) // bx)
@@ -340,6 +346,8 @@ class BrickPlan:
         R = tgt.numel()
         self.n_src = R // kw
         valid = tgt >= 0
+        if mask is not None:
+            valid = valid & mask.reshape(-1)
         r = torch.nonzero(valid).squeeze(1)
         t = tgt[r]
         z = t // (gy * gx)
@@ -348,16 +356,36 @@ class BrickPlan:
         x = rem - y * gx
         brick_id = ((z // bz) * self.nb[1] + (y // by)) * self.nb[2] + (x // bx)
         cl = ((z % bz) * by + (y % by)) * bx + (x % bx)
-        key = brick_id * self.cells + cl
-        key_sorted, order = torch.sort(key, stable=True)
-        r = r[order]
-        brick_sorted = key_sorted // self.cells
-        cl_sorted = key_sorted - brick_sorted * self.cells
+        # sort key (brick, outer table index, cell): runs sharing the outer
+        # factor and the target cell are contiguous inside each brick
+        e_all = interp_idx.reshape(-1)[r].to(torch.int64)
+        kout = e_all % self.n_outer
+        if order == "inner":
+            # (brick, inner index, outer index, cell): a warp's lanes share operators
+            n_in = int(e_all.max()) // self.n_outer + 1 if e_all.numel() else 1
+            key = ((brick_id * n_in + e_all // self.n_outer) * self.n_outer + kout) * self.cells + cl
+            span = n_in * self.n_outer * self.cells
+        else:
+            # (brick, outer index, cell): runs sharing the outer factor and cell
+            key = (brick_id * self.n_outer + kout) * self.cells + cl
+            span = self.n_outer * self.cells
+        key_sorted, perm = torch.sort(key, stable=True)
+        r = r[perm]
+        brick_sorted = key_sorted // span
+        cl_sorted = key_sorted % self.cells
         entry = interp_idx.reshape(-1)[r].to(torch.int64)
         if entry.numel() and int(entry.max()) >= 2**20:
             raise ValueError("shift table too large for the fused kernels (max 2^20 entries)")
         self.rep_src = (r // kw).to(torch.int32).contiguous()
-        self.rep_meta = _u32_to_i32(entry | (cl_sorted << 20)).contiguous()
+        if pack == "split":
+            # cell | inner << 11 | outer << 25  (T[e] = outer[e % n] @ inner[e // n])
+            inner_i = entry // self.n_outer
+            outer_i = entry % self.n_outer
+            if self.cells > 2048 or (entry.numel() and (int(inner_i.max()) >= 16384 or self.n_outer > 128)):
+                raise ValueError("split metadata needs cells <= 2048, inner < 16384, outer <= 128")
+            self.rep_meta = _u32_to_i32(cl_sorted | (inner_i << 11) | (outer_i << 25)).contiguous()
+        else:
+            self.rep_meta = _u32_to_i32(entry | (cl_sorted << 20)).contiguous()
         self.rep_w = rep_weight.reshape(-1)[r].to(torch.float32).contiguous()
         self.n_valid = int(r.numel())
         counts = torch.bincount(brick_sorted, minlength=n_bricks)
@@ -392,33 +420,177 @@ class BrickPlan:
             int(self.split_bricks.numel()),
         )
 
-    def grid_forward(self, data: torch.Tensor, table: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
-        """``out (B, C, G) = fused forward of data (B, C, N)``."""
-        B, C, N = data.shape
-        G = out.shape[-1]
-        _lib.call(
-            "pgb_grog_grid", data.data_ptr(), N, out.data_ptr(), G, table.data_ptr(),
-            table.shape[0], C, B, _ctypes_ref(self._c_all), _lib.stream_ptr(data.device),
-        )
-        return out
-
-    def grid_adjoint(self, grid: torch.Tensor, table_h: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
-        """``out (B, C, N) = adjoint of the fused forward applied to grid (B, C, G)``."""
-        B, C, G = grid.shape
-        N = out.shape[-1]
-        _lib.call(
-            "pgb_grog_degrid", grid.data_ptr(), G, out.data_ptr(), N, table_h.data_ptr(),
-            table_h.shape[0], C, B, _ctypes_ref(self._c_nonempty), 1 if self.multi else 0,
-            self.zero_src.data_ptr() if self.zero_src.numel() else None, int(self.zero_src.numel()),
-            _lib.stream_ptr(grid.device),
-        )
-        return out
-
 
 def _ctypes_ref(s):
     import ctypes
 
     return ctypes.byref(s)
+
+
+_SMEM_BUDGET = 220 * 1024
+_SMEM_V3 = 227 * 1024
+
+
+def _first_valid_mask(target_idx: torch.Tensor, kw: int) -> torch.Tensor:
+    """True for the first valid replica (lowest replica index) of each sample."""
+    tgt = target_idx.reshape(-1, kw)
+    valid = tgt >= 0
+    first = torch.argmax(valid.to(torch.int8), dim=1)  # first True per row (0 if none)
+    m = torch.zeros_like(valid)
+    rows = torch.arange(tgt.shape[0], device=tgt.device)
+    m[rows, first] = True
+    return (m & valid).reshape(-1)
+
+
+class GrogGridder:
+    """Fused GROG gridding operator for one trajectory: brick plans + tables.
+
+    Kernel families (chosen from the shared-memory budget of one CTA):
+      ``"v3"``        C <= 16: whole table or its inner factor in shared
+                      memory, sub-chunks staged ahead in shared memory by
+                      persistent CTAs, adjoint as store pass + atomic pass;
+      ``"smem"`` / ``"factored"``  same tables, one slot pipeline per CTA;
+      ``"global"``    table read through L1/L2 (any C <= 32, K < 2^20).
+    With a factored table ``T[e] = outer[e % n] @ inner[e // n]``, the outer
+    factor is applied once per run of replicas sharing (outer index, cell).
+    """
+
+    BRICKS3 = ((8, 8, 8), (4, 8, 8), (4, 4, 8), (2, 4, 8))
+    BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
+
+    def __init__(self, target_idx, interp_idx, rep_weight, kw, grid_shape, table, factors, nsteps,
+                 mode: str | None = None, brick=None, chunk: int = 2048):
+        C = int(table.shape[-1])
+        K = int(table.shape[0])
+        self.C = C
+        ndim = len(grid_shape)
+        lib = _lib.load_library()
+        cand = self.BRICKS3 if ndim == 3 else self.BRICKS2
+        if brick is not None:
+            cand = (tuple(brick),)
+        n_fact = int(factors[1].shape[0]) if factors is not None else None
+
+        def v3_fits(n_inner, br):
+            cells = br[0] * br[1] * br[2]
+            return (lib.pgb_grog_v3_smem_bytes(C, cells, n_inner, 1) <= _SMEM_V3
+                    and lib.pgb_grog_v3_smem_bytes(C, cells, n_inner, 0) <= _SMEM_V3)
+
+        def v5_fits(n_inner, n_outer, br):
+            cells = br[0] * br[1] * br[2]
+            return lib.pgb_grog_v5_smem_bytes(C, cells, n_inner, n_outer) <= _SMEM_V3
+
+        chosen = None
+        if mode in (None, "v5") and C <= 16:
+            for br in cand:
+                if v5_fits(K, 1, br) and K <= 16384:
+                    chosen = ("v5", br, False)
+                    break
+                if (n_fact is not None and n_fact <= 16384 and int(factors[0].shape[0]) <= 128
+                        and v5_fits(n_fact, int(factors[0].shape[0]), br)):
+                    chosen = ("v5", br, True)
+                    break
+        if chosen is None and mode in (None, "v3") and C <= 16:
+            for br in cand:
+                if v3_fits(K, br):
+                    chosen = ("v3", br, False)
+                    break
+                if n_fact is not None and n_fact <= 16384 and int(factors[0].shape[0]) <= 128 and v3_fits(n_fact, br):
+                    chosen = ("v3", br, True)
+                    break
+        if chosen is None:
+            if mode in ("v3", "v5"):
+                raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
+            br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
+                (4, 8, 8) if ndim == 3 else (1, 16, 16))
+            if brick is not None:
+                br = tuple(brick)
+            cells = br[0] * br[1] * br[2]
+            fit = lambda n: lib.pgb_grog_factored_smem_bytes(C, cells, n) <= _SMEM_BUDGET  # noqa: E731
+            if mode in (None, "smem") and fit(K):
+                chosen = ("smem", br, False)
+            elif mode in (None, "factored") and n_fact is not None and fit(n_fact):
+                chosen = ("factored", br, True)
+            else:
+                chosen = ("global", br, False)
+        self.mode, brick, factored = chosen
+        self.brick = brick
+        dev = target_idx.device
+        if factored:
+            outer, inner = factors
+            self.n_outer = int(outer.shape[0])
+            self.inner = inner.to(dev).contiguous()
+            self.outer = outer.to(dev).contiguous()
+            self.inner_h = self.inner.conj().transpose(-1, -2).contiguous()
+            self.outer_h = self.outer.conj().transpose(-1, -2).contiguous()
+        else:
+            self.n_outer = 1
+            self.inner = torch.as_tensor(table).to(dev).contiguous()
+            self.inner_h = self.inner.conj().transpose(-1, -2).contiguous()
+            self.outer = self.outer_h = None
+        pack = "split" if self.mode in ("v3", "v5") else "wide"
+        kwargs = dict(brick=brick, chunk=chunk, n_outer=self.n_outer, pack=pack,
+                      order="inner" if self.mode == "v5" else "cell")
+        self.plan = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, **kwargs)
+        self.plan2 = None  # adjoint secondary replicas (v3 / v5)
+        self.adj_plan = self.plan
+        if self.mode in ("v3", "v5"):
+            first = _first_valid_mask(target_idx, kw)
+            self.adj_plan = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwargs)
+            if self.plan.n_valid > self.adj_plan.n_valid:
+                self.plan2 = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kwargs)
+
+    @property
+    def n_valid(self):
+        return self.plan.n_valid
+
+    def launches_per_call(self, adjoint: bool) -> int:
+        bp = self.plan
+        if adjoint:
+            if self.mode in ("v3", "v5"):
+                return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
+            return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
+        return 1 + (1 if bp.split_bricks.numel() else 0)
+
+    def _outer_ptr(self, h: bool):
+        t = self.outer_h if h else self.outer
+        return t.data_ptr() if t is not None else None
+
+    def forward(self, data: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out (B, C, G)`` <- fused gridding of ``data (B, C, N)``."""
+        B, C, N = data.shape
+        G = out.shape[-1]
+        bp = self.plan
+        st = _lib.stream_ptr(data.device)
+        if self.mode == "global":
+            _lib.call("pgb_grog_grid", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
+                      self.inner.shape[0], C, B, _ctypes_ref(bp._c_all), st)
+        else:
+            fn = {"v3": "pgb_grog_grid_v3", "v5": "pgb_grog_grid_v5"}.get(self.mode, "pgb_grog_grid_factored")
+            _lib.call(fn, data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(), self.inner.shape[0],
+                      self._outer_ptr(False), self.n_outer, C, B, _ctypes_ref(bp._c_all), st)
+        return out
+
+    def adjoint(self, grid: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out (B, C, N)`` <- adjoint of :meth:`forward` applied to ``grid (B, C, G)``."""
+        B, C, G = grid.shape
+        N = out.shape[-1]
+        bp = self.adj_plan
+        st = _lib.stream_ptr(grid.device)
+        zs = bp.zero_src.data_ptr() if bp.zero_src.numel() else None
+        if self.mode in ("v3", "v5"):
+            sec = _ctypes_ref(self.plan2._c_nonempty) if self.plan2 is not None else None
+            _lib.call("pgb_grog_degrid_v3" if self.mode == "v3" else "pgb_grog_degrid_v5", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
+                      self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,
+                      _ctypes_ref(bp._c_nonempty), sec, zs, int(bp.zero_src.numel()), st)
+        elif self.mode == "global":
+            _lib.call("pgb_grog_degrid", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
+                      self.inner_h.shape[0], C, B, _ctypes_ref(bp._c_nonempty), 1 if bp.multi else 0,
+                      zs, int(bp.zero_src.numel()), st)
+        else:
+            _lib.call("pgb_grog_degrid_factored", grid.data_ptr(), G, out.data_ptr(), N,
+                      self.inner_h.data_ptr(), self.inner_h.shape[0], self._outer_ptr(True), self.n_outer,
+                      C, B, _ctypes_ref(bp._c_nonempty), 1 if bp.multi else 0, zs, int(bp.zero_src.numel()), st)
+        return out
 
 
 # ---------------------------------------------------------------------------
@@ -488,7 +660,11 @@ class GrogInterpolator:
         """
         if isinstance(train_data, torch.Tensor):
             train_data = train_data.detach().cpu()
-        table, nsteps, ndim = KernelTable(train_data, self.plan.radius, precision, lamda, fit_dtype)
+        table, nsteps, ndim, factors = KernelTable(
+            train_data, self.plan.radius, precision, lamda, fit_dtype, return_factors=True
+        )
+        self._factors = factors
+        self._nsteps = int(nsteps)
         dist = self.plan.distances
         if dist is None:
             raise RuntimeError("calc_interp_table: plan distances were already released")
@@ -553,7 +729,7 @@ class GrogInterpolator:
         batch = tuple(int(s) for s in data.shape[: cpos - s_ndim])
         return batch, s_shape, int(data.shape[cpos]), spatial, kw
 
-    def _brick(self, s: int) -> BrickPlan:
+    def _brick(self, s: int) -> "GrogGridder":
         if self._brick_plans is None:
             self._brick_plans = {}
         bp = self._brick_plans.get(s)
@@ -566,7 +742,8 @@ class GrogInterpolator:
             sw = torch.sqrt(w)
             rep_w = sw * sw
             idx = self._interp_idx.reshape(s_total, -1)[s]
-            bp = BrickPlan(tgt, idx, rep_w, kw, plan.grid_shape)
+            bp = GrogGridder(tgt, idx, rep_w, kw, plan.grid_shape, self._interp_kernel, self._factors,
+                             self._nsteps, mode=getattr(self, "gridder_mode", None))
             self._brick_plans[s] = bp
         return bp
 
@@ -671,7 +848,7 @@ class GrogInterpolator:
             bp = self._brick(s)
             ds = d[:, s].contiguous()
             o = torch.empty(B, C, G, dtype=data.dtype, device=data.device) if S > 1 else out.view(B, C, G)
-            bp.grid_forward(ds, self._table_d, o)
+            bp.forward(ds, o)
             if S > 1:
                 out[:, s] = o
         density = self._density_grid()
@@ -700,7 +877,7 @@ class GrogInterpolator:
         for s in range(S):
             ds = d[:, s].contiguous()
             o = torch.empty(B, C, G, dtype=t.dtype, device=t.device) if S > 1 else out.view(B, C, G)
-            self._brick(s).grid_forward(ds, self._table_d, o)
+            self._brick(s).forward(ds, o)
             if S > 1:
                 out[:, s] = o
         res = out.reshape(*batch, *s_shape, C, *plan.grid_shape)
@@ -736,7 +913,7 @@ class GrogInterpolator:
         for s in range(S):
             gs = g[:, s].contiguous()
             o = torch.empty(B, C, N, dtype=t.dtype, device=t.device) if S > 1 else out.view(B, C, N)
-            self._brick(s).grid_adjoint(gs, self._table_h_d, o)
+            self._brick(s).adjoint(gs, o)
             if S > 1:
                 out[:, s] = o
         res = out.reshape(*batch, *s_shape, C, *spatial)

@@ -95,3 +95,32 @@ def test_brick_plan_covers_every_valid_replica_once(shape):
     key = brick_of * bp.cells + cl
     assert np.all(np.diff(key) >= 0)
     assert bp.multi == bool(np.bincount(r_sorted // 3).max() > 1)
+
+
+def test_brick_plan_split_packing_and_first_valid_mask():
+    rng = np.random.default_rng(3)
+    shape = (24, 16, 40)
+    kw = 4
+    tgt, idx, w = _toy_plan(shape, 2000, kw, rng)
+    idx = torch.from_numpy(rng.integers(0, 11 * 121, size=(2000, kw)).astype(np.int64))
+    bp = _grog.BrickPlan(tgt, idx, w, kw, shape, brick=(4, 8, 8), n_outer=11, pack="split")
+    meta = bp.rep_meta.numpy().astype(np.int64) & 0xFFFFFFFF
+    cl = meta & 2047
+    inner = (meta >> 11) & 16383
+    outer = meta >> 25
+    r = np.nonzero(tgt.numpy().reshape(-1) >= 0)[0]
+    e_all = idx.numpy().reshape(-1)
+    got = sorted(zip(bp.rep_src.numpy().tolist(), (inner * 11 + outer).tolist()))
+    exp = sorted(zip((r // kw).tolist(), e_all[r].tolist()))
+    assert got == exp
+    assert np.all(cl < bp.cells)
+    # inside each work item, replicas are ordered by (outer index, cell)
+    for row in bp.work.numpy():
+        key = outer[row[1]:row[2]] * bp.cells + cl[row[1]:row[2]]
+        assert np.all(np.diff(key) >= 0)
+    first = _grog._first_valid_mask(tgt, kw).numpy().reshape(-1, kw)
+    valid = tgt.numpy() >= 0
+    assert np.array_equal(first.sum(1), valid.any(1).astype(int))
+    for n in range(0, 2000, 37):
+        if valid[n].any():
+            assert first[n, np.argmax(valid[n])]
