@@ -258,6 +258,72 @@ PGB_API int pgb_grog_expand(const void* data, int64_t N, int kw, const int64_t* 
                     const void* table, int64_t K, int64_t C, int64_t B, void* out,
                     void* stream);
 
+/* =====================================================================
+ * SparseFFT / MaskedFFT / Toeplitz stages around cuFFT
+ * (operator/_sparse_fft.py:574-621, 741-789, 1154-1177;
+ *  operator/_masked_fft.py:322-430; _toep/_grog_toep.py:154-209;
+ *  _base/_fftc.py:114-139)
+ * Buffers handed to cuFFT are in "FFT order": centred grid index p (per
+ * axis, extent g) is stored at m = (p - g/2) mod g, which is exactly
+ * ifftshift, so no shift pass is ever made.  grid_shape / image_shape are
+ * HOST arrays of ndim (2 or 3) extents; all other pointers are device
+ * pointers; complex data are complex64.
+ * ===================================================================== */
+
+/* u[b,c,m] = scale * S[c,q(m)] * x[b,q(m)] (x_has_coils = 0, smaps may be
+ * NULL for a single coil) or scale * x[b,c,q(m)] (x_has_coils = 1); zero
+ * outside the centred image: zero-pad + coil expansion + ifftshift. */
+PGB_API int pgb_fft_expand(const void* x, const void* smaps, void* u, int64_t B, int64_t C,
+                           int ndim, const int64_t* grid_shape, const int64_t* image_shape,
+                           float scale, int x_has_coils, void* stream);
+
+/* out[b,q] = scale * sum_c conj(S[c,q]) v[b,c,m(q)] (smaps) or
+ * out[b,c,q] = scale * v[b,c,m(q)] (smaps NULL); plus add_scale * add[...]
+ * when add is not NULL: fftshift + crop + coil combine (+ damping term). */
+PGB_API int pgb_fft_combine(const void* v, const void* smaps, void* out, int64_t B, int64_t C,
+                            int ndim, const int64_t* grid_shape, const int64_t* image_shape,
+                            float scale, const void* add, float add_scale, void* stream);
+
+/* u[bc, cellpos[r]] += w[r] * data[bc, r] for bc < BC (u pre-zeroed by the
+ * caller); entries with cellpos outside [0,G) or w == 0 are skipped. */
+PGB_API int pgb_sparse_scatter(const void* data, const int32_t* cellpos, const float* w, void* u,
+                               int64_t BC, int64_t R, int64_t G, void* stream);
+
+/* out[bc, r] = w[r] * U[bc, cellpos[r]] (0 for cellpos outside [0,G)). */
+PGB_API int pgb_sparse_gather(const void* U, const int32_t* cellpos, const float* w, void* out,
+                              int64_t BC, int64_t R, int64_t G, void* stream);
+
+/* U[bc, m] *= psf[m] (real PSF in FFT order; Toeplitz normal operator). */
+PGB_API int pgb_psf_apply(void* U, const float* psf, int64_t BC, int64_t G, void* stream);
+
+/* to_centred = 0: dst[bc,m] = scale * mask[p(m)] * src[bc,p(m)];
+ * to_centred = 1: dst[bc,p] = scale * mask[p] * src[bc,m(p)]  (mask may be
+ * NULL).  src and dst must not alias. */
+PGB_API int pgb_fft_shift(const void* src, const float* mask, void* dst, int64_t BC, int ndim,
+                          const int64_t* grid_shape, float scale, int to_centred, void* stream);
+
+/* =====================================================================
+ * Conjugate gradient scalars in FP64 on the device (_solve/_solvers.py:49-139)
+ * scalars: double[8] = {rz_old, pAp, rr, r0_norm, rel, done, tol, spare}
+ * scratch: pgb_reduce_scratch_bytes() bytes, zero-initialised once; its
+ * counters return to zero after every call.  Every kernel is a no-op once
+ * done != 0, which replaces the host-side early exit.
+ * ===================================================================== */
+PGB_API size_t pgb_reduce_scratch_bytes(void);
+/* mode 0: scalars[out_slot] = sum Re(conj(a) b) (b NULL: |a|^2);
+ * mode 1: rr = |a|^2, rel = sqrt(rr)/r0_norm, done |= rel < tol;
+ * mode 2: CG start: rr = rz_old = |a|^2, r0_norm = sqrt(rr) + 1e-30. */
+PGB_API int pgb_dot_f64(const void* a, const void* b, int64_t n, void* scratch, void* scalars,
+                        int out_slot, int mode, void* stream);
+/* alpha = rz_old / (pAp + 1e-30); x += alpha p; r -= alpha Ap */
+PGB_API int pgb_cg_update_xr(void* x, void* r, const void* p, const void* Ap, int64_t n,
+                             const void* scalars, void* stream);
+/* beta = rr / (rz_old + 1e-30); p = r + beta p; rz_old = rr */
+PGB_API int pgb_cg_update_p(void* p, const void* r, int64_t n, void* scalars, void* scratch,
+                            void* stream);
+/* y += a x */
+PGB_API int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,112 @@
+"""Oracle: CPU restatement of the reference Cartesian operators (numpy).
+
+TEST INFRASTRUCTURE ONLY (never imported by the product).  Parity pinned by
+``tests/test_oracle_golden.py`` against fixtures produced by the reference
+itself (``tests/golden/ops_*.npz``).
+
+References (FiRMLAB-Pisa/pygrog):
+  centred ortho FFT           _base/_fftc.py:114-139
+  SparseFFT adjoint / forward operator/_sparse_fft.py:574-621, 741-789, 1154-1177
+  Toeplitz normal             _toep/_grog_toep.py:154-209
+  MaskedFFT                   operator/_masked_fft.py:322-430
+  CG                          _solve/_solvers.py:49-139
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def fftc(x, axes):
+    return np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho"), axes=axes)
+
+
+def ifftc(x, axes):
+    return np.fft.fftshift(np.fft.ifftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho"), axes=axes)
+
+
+def _slices(grid_shape, image_shape):
+    return tuple(slice((g - i) // 2, (g - i) // 2 + i) for g, i in zip(grid_shape, image_shape))
+
+
+def sparse_adjoint(sparse, idx_nat, sw_nat, grid_shape, image_shape, smaps=None):
+    """sparse (C, R) natural order -> image (*img) with smaps, else (C, *img)."""
+    C = sparse.shape[0]
+    G = int(np.prod(grid_shape))
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    grid = np.zeros((C, G), dtype=np.complex128)
+    for c in range(C):
+        np.add.at(grid[c], idx_nat, sw_nat * sparse[c])
+    img = ifftc(grid.reshape(C, *grid_shape), axes)[(slice(None), *_slices(grid_shape, image_shape))]
+    if smaps is None:
+        return img
+    return (np.conj(smaps) * img).sum(0)
+
+
+def sparse_forward(image, idx_nat, sw_nat, grid_shape, image_shape, smaps=None):
+    """image (*img) [smaps] or (C, *img) -> sparse (C, R) natural order."""
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    coil = smaps * image if smaps is not None else image
+    C = coil.shape[0]
+    pad = np.zeros((C, *grid_shape), dtype=np.complex128)
+    pad[(slice(None), *_slices(grid_shape, image_shape))] = coil
+    k = fftc(pad, axes).reshape(C, -1)
+    return sw_nat * k[:, idx_nat]
+
+
+def psf(idx_nat, sw_nat, grid_shape):
+    p = np.zeros(int(np.prod(grid_shape)), dtype=np.float64)
+    np.add.at(p, idx_nat, sw_nat.astype(np.float64) ** 2)
+    return p.reshape(grid_shape)
+
+
+def toeplitz_normal(x, psf_grid, grid_shape, image_shape, smaps=None):
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    coil = smaps * x if smaps is not None else x
+    C = coil.shape[0]
+    pad = np.zeros((C, *grid_shape), dtype=np.complex128)
+    sl = (slice(None), *_slices(grid_shape, image_shape))
+    pad[sl] = coil
+    img = ifftc(psf_grid * fftc(pad, axes), axes)[sl]
+    if smaps is None:
+        return img
+    return (np.conj(smaps) * img).sum(0)
+
+
+def masked_adjoint(kgrid, mask, grid_shape, image_shape, smaps=None):
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    img = ifftc(kgrid * mask, axes)[(slice(None), *_slices(grid_shape, image_shape))]
+    return img if smaps is None else (np.conj(smaps) * img).sum(0)
+
+
+def masked_forward(image, mask, grid_shape, image_shape, smaps=None):
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    coil = smaps * image if smaps is not None else image
+    pad = np.zeros((coil.shape[0], *grid_shape), dtype=np.complex128)
+    pad[(slice(None), *_slices(grid_shape, image_shape))] = coil
+    return fftc(pad, axes) * mask
+
+
+def cg(normal, AHb, damp=0.0, max_iter=20, tol=0.0):
+    """_solvers.py:49-139 in complex128 (x0 = 0, no preconditioner)."""
+    x = np.zeros_like(AHb)
+    r = AHb.copy()
+    p = r.copy()
+    rz = np.vdot(r, r).real
+    r0 = np.linalg.norm(r) + 1e-30
+    for _ in range(max_iter):
+        Ap = normal(p) + damp * p
+        alpha = rz / (np.vdot(p, Ap).real + 1e-30)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        if np.linalg.norm(r) / r0 < tol:
+            break
+        rz_new = np.vdot(r, r).real
+        p = r + rz_new / (rz + 1e-30) * p
+        rz = rz_new
+    return x

@@ -12,7 +12,5 @@ from ._lib import load_library  # noqa: F401
 
 __version__ = "0.1.0"
 
-try:
-    from ._solve import cg, lsmr, solve  # noqa: F401
-except ImportError:  # pragma: no cover
-    pass
+from ._solve import cg, lsmr, solve  # noqa: F401
+from ._toep import GrogToeplitzOp  # noqa: F401

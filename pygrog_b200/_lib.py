@@ -87,11 +87,22 @@ _SIGS = {
         _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC),
         ctypes.POINTER(BrickPlanC), _vp, _i64, _vp,
     ],
+    "pgb_fft_expand": [_vp, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _f32, _i32, _vp],
+    "pgb_fft_combine": [_vp, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _f32, _vp, _f32, _vp],
+    "pgb_sparse_scatter": [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _vp],
+    "pgb_sparse_gather": [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _vp],
+    "pgb_psf_apply": [_vp, _vp, _i64, _i64, _vp],
+    "pgb_fft_shift": [_vp, _vp, _vp, _i64, _i32, _vp, _f32, _i32, _vp],
+    "pgb_dot_f64": [_vp, _vp, _i64, _vp, _vp, _i32, _i32, _vp],
+    "pgb_cg_update_xr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp],
+    "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
+    "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
 }
 _SIZE_FUNCS = {
     "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],
     "pgb_grog_v3_smem_bytes": [_i64, _i64, _i64, _i32],
     "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
+    "pgb_reduce_scratch_bytes": [],
 }
 
 _lib = None

@@ -1,0 +1,305 @@
+"""Iterative solvers: CG with device-side FP64 scalars, LSMR, ``solve``.
+
+Mirrors ``_solve/_solvers.py`` (``cg`` 49-139, ``lsmr`` 145-262, ``solve``
+268-302) and ``_solve/_mixin.py`` (``SolveMixin`` 84-158) of
+FiRMLAB-Pisa/pygrog.
+
+CG on an operator of this package runs as a fixed sequence of kernels per
+iteration -- ``Ap = A^H A p + damp p`` (Toeplitz or fused forward/adjoint),
+FP64 ``<p, Ap>``, x/r update, FP64 ``|r|^2`` with the relative-residual test,
+p update -- with every scalar kept in device memory and a device flag
+replacing the host-side ``break``.  Without a callback one iteration is
+captured in a CUDA graph and replayed ``max_iter`` times: no host
+synchronisation inside the loop.  Other duck-typed operators use the
+reference recurrence with torch tensors (inner products in FP64).
+"""
+
+from __future__ import annotations
+
+__all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG"]
+
+from collections.abc import Callable
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _normalize_kspace_shape(op: Any, b: torch.Tensor) -> torch.Tensor:
+    nat = getattr(op, "natural_shape", None)
+    if nat is None or len(nat) <= 1:
+        return b
+    nat = tuple(int(s) for s in nat)
+    n = int(np.prod(nat))
+    if b.shape[-1] != n:
+        return b
+    return b.reshape(*b.shape[:-1], *nat)
+
+
+def _vdot_re64(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    return torch.vdot(a.reshape(-1).to(torch.complex128), b.reshape(-1).to(torch.complex128)).real
+
+
+class DeviceCG:
+    """CG state for one frame on the device (FP64 scalars, optional CUDA graph)."""
+
+    def __init__(self, op, AHb: torch.Tensor, damp: float, tol: float, x0=None):
+        self.op = op
+        dev = AHb.device
+        self.damp = float(damp)
+        self.x = torch.zeros_like(AHb) if x0 is None else x0.to(dev, torch.complex64).clone()
+        self.Ap = torch.empty_like(AHb)
+        if x0 is None:
+            self.r = AHb.clone()
+        else:
+            op._normal_into(self.x, self.Ap, self.damp)
+            self.r = AHb - self.Ap
+        self.p = self.r.clone()
+        self.n = int(AHb.numel())
+        lib = _lib.load_library()
+        nbytes = int(lib.pgb_reduce_scratch_bytes())
+        self.scratch = torch.zeros((nbytes + 7) // 8, dtype=torch.float64, device=dev)
+        self.scal = torch.zeros(8, dtype=torch.float64, device=dev)
+        self.scal[6] = float(tol)
+        st = _lib.stream_ptr(dev)
+        _lib.call("pgb_dot_f64", self.r.data_ptr(), None, self.n, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 0, 2, st)
+        self.graph = None
+
+    def step(self):
+        st = _lib.stream_ptr(self.p.device)
+        self.op._normal_into(self.p, self.Ap, self.damp)
+        _lib.call("pgb_dot_f64", self.p.data_ptr(), self.Ap.data_ptr(), self.n, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 1, 0, st)
+        _lib.call("pgb_cg_update_xr", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
+                  self.Ap.data_ptr(), self.n, self.scal.data_ptr(), st)
+        _lib.call("pgb_dot_f64", self.r.data_ptr(), None, self.n, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 2, 1, st)
+        _lib.call("pgb_cg_update_p", self.p.data_ptr(), self.r.data_ptr(), self.n, self.scal.data_ptr(),
+                  self.scratch.data_ptr(), st)
+
+    def capture(self):
+        """Capture one iteration in a CUDA graph (after a warm-up of the FFT plans)."""
+        side = torch.cuda.Stream(self.p.device)
+        side.wait_stream(torch.cuda.current_stream(self.p.device))
+        saved = [t.clone() for t in (self.x, self.r, self.p, self.scal)]
+        with torch.cuda.stream(side):
+            self.step()  # warm-up: cuFFT plans and workspaces exist before capture
+        torch.cuda.current_stream(self.p.device).wait_stream(side)
+        for t, v in zip((self.x, self.r, self.p, self.scal), saved):
+            t.copy_(v)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.step()
+        self.graph = g
+
+    def run(self, max_iter: int, callback: Callable | None = None, use_graph: bool = True):
+        if callback is None and use_graph and max_iter > 1:
+            self.capture()
+            for _ in range(max_iter):
+                self.graph.replay()
+            return self.x
+        for k in range(max_iter):
+            self.step()
+            if callback is not None or self.scal[6] > 0:
+                rel = float(self.scal[4].item())
+                if callback is not None:
+                    callback(k, self.x, rel)
+                if self.scal[5].item() != 0.0:
+                    break
+        return self.x
+
+
+def _device_cg_applicable(op, AHb, preconditioner) -> bool:
+    return (
+        preconditioner is None
+        and hasattr(op, "_normal_into")
+        and isinstance(AHb, torch.Tensor)
+        and AHb.device.type == "cuda"
+        and AHb.dtype == torch.complex64
+        and not getattr(op, "stack_shape", ())
+        and AHb.ndim == len(op.image_shape) + (0 if getattr(op, "smaps", None) is not None else 1)
+    )
+
+
+def cg(
+    op: Any,
+    b: torch.Tensor,
+    *,
+    damp: float = 0.0,
+    x0: torch.Tensor | None = None,
+    max_iter: int = 20,
+    tol: float = 1e-6,
+    preconditioner: Any | None = None,
+    callback: Callable | None = None,
+    use_graph: bool = True,
+) -> torch.Tensor:
+    """CG on ``(A^H A + damp I) x = A^H b`` (``forward = A``, ``adjoint = A^H``)."""
+    b = _normalize_kspace_shape(op, b)
+    src_dev = b.device
+    if hasattr(op, "_cdev") and src_dev.type != "cuda":
+        b = b.to(op._cdev)
+    AHb = op.adjoint(b)
+    if _device_cg_applicable(op, AHb, preconditioner):
+        x0d = None if x0 is None else torch.as_tensor(x0).to(AHb.device)
+        solver = DeviceCG(op, AHb, damp, tol, x0d)
+        x = solver.run(int(max_iter), callback, use_graph)
+        return x.to(src_dev)
+    # generic duck-typed operators: reference recurrence, FP64 inner products
+    AHA = getattr(op, "normal", None)
+    if AHA is None:
+
+        def AHA(v):
+            return op.adjoint(op.forward(v))
+
+    x = torch.zeros_like(AHb) if x0 is None else torch.as_tensor(x0).clone()
+    r = AHb - AHA(x) - damp * x
+    z = preconditioner.apply(r) if preconditioner is not None else r
+    p = z.clone()
+    rz_old = _vdot_re64(r, z)
+    r0 = torch.linalg.vector_norm(r.to(torch.complex128)) + 1e-30
+    for k in range(max_iter):
+        Ap = AHA(p) + damp * p
+        alpha = (rz_old / (_vdot_re64(p, Ap) + 1e-30)).to(torch.float32)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        rel = float((torch.linalg.vector_norm(r.to(torch.complex128)) / r0).item())
+        if callback is not None:
+            callback(k, x, rel)
+        if rel < tol:
+            break
+        z = preconditioner.apply(r) if preconditioner is not None else r
+        rz_new = _vdot_re64(r, z)
+        beta = (rz_new / (rz_old + 1e-30)).to(torch.float32)
+        p = z + beta * p
+        rz_old = rz_new
+    return x.to(src_dev) if isinstance(x, torch.Tensor) else x
+
+
+def lsmr(
+    op: Any,
+    b: torch.Tensor,
+    *,
+    damp: float = 0.0,
+    x0: torch.Tensor | None = None,
+    max_iter: int = 20,
+    atol: float = 1e-6,
+    btol: float = 1e-6,
+    callback: Callable | None = None,
+) -> torch.Tensor:
+    """LSMR (Fong & Saunders) for ``argmin ||A x - b||^2 + damp^2 ||x||^2``.
+
+    The recurrence of the reference (``_solvers.py:145-262``) with FP64
+    norms; vectors stay on the device.
+    """
+    b = _normalize_kspace_shape(op, b)
+    src_dev = b.device
+    if hasattr(op, "_cdev") and src_dev.type != "cuda":
+        b = b.to(op._cdev)
+    if x0 is not None:
+        b = b - op.forward(torch.as_tensor(x0).to(b.device))
+
+    def nrm(t):
+        return torch.linalg.vector_norm(t.to(torch.complex128)).to(torch.float32)
+
+    beta = nrm(b)
+    if beta.item() == 0:
+        out = torch.as_tensor(x0).clone() if x0 is not None else op.adjoint(b)
+        return out.to(src_dev)
+    u = b / beta
+    v_full = op.adjoint(u)
+    alpha = nrm(v_full)
+    if alpha.item() == 0:
+        out = torch.as_tensor(x0).clone() if x0 is not None else torch.zeros_like(v_full)
+        return out.to(src_dev)
+    v = v_full / alpha
+    zetabar = alpha * beta
+    alphabar = alpha
+    one = torch.tensor(1.0, dtype=alpha.dtype, device=alpha.device)
+    rho = one.clone()
+    rhobar = one.clone()
+    cbar = one.clone()
+    sbar = torch.zeros_like(one)
+    h = v.clone()
+    hbar = torch.zeros_like(v)
+    x = torch.zeros_like(v) if x0 is None else torch.as_tensor(x0).to(v.device).clone()
+    normb = beta.clone()
+    zeta = zetabar
+    for k in range(max_iter):
+        u = op.forward(v) - alpha * u
+        beta = nrm(u)
+        if beta.item() > 0:
+            u = u / beta
+            v_full = op.adjoint(u) - beta * v
+            alpha = nrm(v_full)
+            if alpha.item() > 0:
+                v = v_full / alpha
+        alphahat = torch.sqrt(alphabar * alphabar + damp * damp)
+        rhoold = rho.clone()
+        rho = torch.sqrt(alphahat * alphahat + beta * beta)
+        c = alphahat / rho
+        s = beta / rho
+        thetanew = s * alpha
+        alphabar = c * alpha
+        rhobarold = rhobar.clone()
+        thetabar = sbar * rho
+        rhotemp = cbar * rho
+        rhobar = torch.sqrt(rhotemp * rhotemp + thetanew * thetanew)
+        cbar = rhotemp / rhobar
+        sbar = thetanew / rhobar
+        zeta = cbar * zetabar
+        zetabar = -sbar * zetabar
+        hbar = h - (thetabar * rho / (rhoold * rhobarold)) * hbar
+        x = x + (zeta / (rho * rhobar)) * hbar
+        h = v - (thetanew / rho) * h
+        rel = (torch.abs(zetabar) / (normb + 1e-30)).item()
+        if callback is not None:
+            callback(k, x, rel)
+        if rel < atol + btol:
+            break
+    return x.to(src_dev)
+
+
+def solve(op: Any, b: torch.Tensor, *, method: str = "cg", **kwargs) -> torch.Tensor:
+    """Dispatch to :func:`cg` or :func:`lsmr` (reference ``solve``)."""
+    method = method.lower()
+    if method == "cg":
+        return cg(op, b, **kwargs)
+    if method == "lsmr":
+        return lsmr(op, b, **kwargs)
+    raise ValueError(f"Unknown solver method: {method!r}. Use 'cg' or 'lsmr'.")
+
+
+def _backend(x) -> str:
+    if isinstance(x, torch.Tensor):
+        return "torch"
+    if isinstance(x, np.ndarray):
+        return "numpy"
+    return "torch"
+
+
+class SolveMixin:
+    """``op.solve(b, method=None, damp, x0, max_iter, tol, preconditioner, callback)``.
+
+    ``method=None`` picks ``cg`` when ``self.toeplitz`` else ``lsmr`` (reference
+    ``_mixin.py:131-132``); numpy inputs give numpy outputs.
+    """
+
+    def solve(self, b, *, method=None, damp=0.0, x0=None, max_iter=20, tol=1e-6, preconditioner=None,
+              callback=None, **kwargs):
+        backend = _backend(b)
+        b_t = torch.as_tensor(b)
+        x0_t = None if x0 is None else torch.as_tensor(x0)
+        if method is None:
+            method = "cg" if getattr(self, "toeplitz", False) else "lsmr"
+        method = method.lower()
+        if method == "cg":
+            out = cg(self, b_t, damp=damp, x0=x0_t, max_iter=max_iter, tol=tol, preconditioner=preconditioner,
+                     callback=callback, **kwargs)
+        elif method == "lsmr":
+            out = lsmr(self, b_t, damp=damp, x0=x0_t, max_iter=max_iter, callback=callback, **kwargs)
+        else:
+            raise ValueError(f"Unknown method: {method!r}")
+        return out.detach().cpu().numpy() if backend == "numpy" else out

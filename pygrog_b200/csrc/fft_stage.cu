@@ -1,1 +1,305 @@
+// fft_stage.cu -- pointwise stages around cuFFT for SparseFFT / MaskedFFT /
+// the GROG Toeplitz normal operator.
+//
+// Reference: operator/_sparse_fft.py:574-621, 741-789, 1154-1177 (per-coil
+// scatter -> centred IFFT -> crop -> conj-smaps accumulate, and smaps ->
+// pad -> centred FFT -> gather -> unsort), operator/_masked_fft.py:
+// 322-361, 408-430, _toep/_grog_toep.py:154-209, _base/_fftc.py:114-139.
+//
+// Centred transforms fftshift(fft(ifftshift(.))) are never materialised:
+// the buffers handed to cuFFT are kept in "FFT order", where centred grid
+// position p (per axis, extent g) sits at m = (p - g/2) mod g.  Padding,
+// cropping, shifting, the coil-sensitivity multiply, the coil sum and the
+// ortho scale all happen inside these kernels, so each stage is one pass
+// over the coil grids instead of the reference's pad / shift / multiply /
+// shift / crop / accumulate passes per coil.
 #include "common.cuh"
+
+namespace pgb {
+
+struct Shape3 {
+  int nd;        // 2 or 3 (2-D uses axis 0 = 1)
+  int g[3];      // grid extent per axis (z, y, x)
+  int n[3];      // image extent per axis
+  int off[3];    // (g - n) / 2 : image origin inside the centred grid
+};
+
+__device__ __forceinline__ void unflat3(int64_t t, const int* e, int& a, int& b, int& c) {
+  c = static_cast<int>(t % e[2]);
+  const int64_t u = t / e[2];
+  b = static_cast<int>(u % e[1]);
+  a = static_cast<int>(u / e[1]);
+}
+
+// FFT-order index m -> centred index p (per axis)
+__device__ __forceinline__ int m2p(int m, int g) {
+  int p = m + g / 2;
+  return p >= g ? p - g : p;
+}
+// centred index p -> FFT-order index m
+__device__ __forceinline__ int p2m(int p, int g) {
+  int m = p - g / 2;
+  return m < 0 ? m + g : m;
+}
+
+// u[b, c, m] = scale * S[c, q] * x[b, q]   (or x[b, c, q] without smaps)
+// for every FFT-order grid position m; zero outside the image.
+__global__ void fft_expand_kernel(const float2* __restrict__ x, const float2* __restrict__ smaps,
+                                  float2* __restrict__ u, int B, int C, Shape3 s, float scale,
+                                  int x_has_coils) {
+  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
+  const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
+  const int64_t total = static_cast<int64_t>(B) * C * G;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t m = t % G;
+    const int64_t bc = t / G;
+    const int c = static_cast<int>(bc % C);
+    const int b = static_cast<int>(bc / C);
+    int m0, m1, m2;
+    unflat3(m, s.g, m0, m1, m2);
+    const int q0 = m2p(m0, s.g[0]) - s.off[0];
+    const int q1 = m2p(m1, s.g[1]) - s.off[1];
+    const int q2 = m2p(m2, s.g[2]) - s.off[2];
+    float2 v = make_float2(0.f, 0.f);
+    if (q0 >= 0 && q0 < s.n[0] && q1 >= 0 && q1 < s.n[1] && q2 >= 0 && q2 < s.n[2]) {
+      const int64_t q = (static_cast<int64_t>(q0) * s.n[1] + q1) * s.n[2] + q2;
+      if (x_has_coils) {
+        v = x[(static_cast<int64_t>(b) * C + c) * I + q];
+      } else {
+        v = x[static_cast<int64_t>(b) * I + q];
+        if (smaps) v = cmul(v, smaps[static_cast<int64_t>(c) * I + q]);
+      }
+      v = cscale(v, scale);
+    }
+    u[t] = v;
+  }
+}
+
+// out[b, q] = scale * sum_c conj(S[c, q]) v[b, c, m(q)]   (smaps)
+// out[b, c, q] = scale * v[b, c, m(q)]                      (no smaps)
+// optionally + add_scale * add[b, (c,) q]  (damped normal equations).
+__global__ void fft_combine_kernel(const float2* __restrict__ v, const float2* __restrict__ smaps,
+                                   float2* __restrict__ out, int B, int C, Shape3 s, float scale,
+                                   const float2* __restrict__ add, float add_scale) {
+  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
+  const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
+  const int Cout = smaps ? 1 : C;
+  const int64_t total = static_cast<int64_t>(B) * Cout * I;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q = t % I;
+    const int64_t bc = t / I;
+    int q0, q1, q2;
+    unflat3(q, s.n, q0, q1, q2);
+    const int64_t m = (static_cast<int64_t>(p2m(q0 + s.off[0], s.g[0])) * s.g[1] +
+                       p2m(q1 + s.off[1], s.g[1])) * s.g[2] + p2m(q2 + s.off[2], s.g[2]);
+    float2 acc = make_float2(0.f, 0.f);
+    if (smaps) {
+      const int64_t b = bc;
+      for (int c = 0; c < C; ++c)
+        cfma_conj(acc, smaps[static_cast<int64_t>(c) * I + q], v[(b * C + c) * G + m]);
+    } else {
+      acc = v[bc * G + m];
+    }
+    acc = cscale(acc, scale);
+    if (add) {
+      const float2 a = add[t];
+      acc.x = fmaf(add_scale, a.x, acc.x);
+      acc.y = fmaf(add_scale, a.y, acc.y);
+    }
+    out[t] = acc;
+  }
+}
+
+// u[b, c, cellpos[r]] += w[r] * data[b, c, r]  (warp-aggregated atomics; u zeroed by caller)
+__global__ void __launch_bounds__(256) sparse_scatter_kernel(const float2* __restrict__ data,
+                                                             const int32_t* __restrict__ cellpos,
+                                                             const float* __restrict__ w,
+                                                             float2* __restrict__ u, int BC, int64_t R,
+                                                             int64_t G) {
+  const int64_t total = static_cast<int64_t>(BC) * R;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < total; base += stride) {
+    const int64_t t = base + threadIdx.x;
+    int64_t key = -1;
+    float2 val = make_float2(0.f, 0.f);
+    if (t < total) {
+      const int64_t r = t % R;
+      const int64_t bc = t / R;
+      const int32_t cp = cellpos[r];
+      const float ww = w[r];
+      if (cp >= 0 && cp < G && ww != 0.f) {
+        key = bc * G + cp;
+        val = cscale(data[t], ww);
+      }
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, key >= 0);
+    if (key >= 0) warp_aggregated_add(u, key, val, active);
+  }
+}
+
+// out[b, c, r] = w[r] * U[b, c, cellpos[r]]
+__global__ void sparse_gather_kernel(const float2* __restrict__ U, const int32_t* __restrict__ cellpos,
+                                     const float* __restrict__ w, float2* __restrict__ out, int BC,
+                                     int64_t R, int64_t G) {
+  const int64_t total = static_cast<int64_t>(BC) * R;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = t % R;
+    const int64_t bc = t / R;
+    const int32_t cp = cellpos[r];
+    float2 v = make_float2(0.f, 0.f);
+    if (cp >= 0 && cp < G) v = cscale(U[bc * G + cp], w[r]);
+    out[t] = v;
+  }
+}
+
+// U[bc, m] *= psf[m]  (real point-spread function in FFT order)
+__global__ void psf_apply_kernel(float2* __restrict__ U, const float* __restrict__ psf, int BC, int64_t G) {
+  const int64_t total = static_cast<int64_t>(BC) * G;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    U[t] = cscale(U[t], psf[t % G]);
+}
+
+// dst[bc, m] = scale * mask[p(m)] * src[bc, p(m)]   (centred -> FFT order)
+// dst[bc, p] = scale * mask[p] * src[bc, m(p)]      (FFT order -> centred), to_centred = 1
+__global__ void fft_shift_kernel(const float2* __restrict__ src, const float* __restrict__ mask,
+                                 float2* __restrict__ dst, int BC, Shape3 s, float scale, int to_centred) {
+  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
+  const int64_t total = static_cast<int64_t>(BC) * G;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = t % G;
+    const int64_t bc = t / G;
+    int a0, a1, a2;
+    unflat3(i, s.g, a0, a1, a2);
+    int64_t j;
+    if (to_centred) {
+      j = (static_cast<int64_t>(p2m(a0, s.g[0])) * s.g[1] + p2m(a1, s.g[1])) * s.g[2] + p2m(a2, s.g[2]);
+      const float mk = mask ? mask[i] : 1.f;
+      dst[t] = cscale(src[bc * G + j], scale * mk);
+    } else {
+      j = (static_cast<int64_t>(m2p(a0, s.g[0])) * s.g[1] + m2p(a1, s.g[1])) * s.g[2] + m2p(a2, s.g[2]);
+      const float mk = mask ? mask[j] : 1.f;
+      dst[t] = cscale(src[bc * G + j], scale * mk);
+    }
+  }
+}
+
+static int make_shape(int nd, const int64_t* grid, const int64_t* image, Shape3& s, const char* who) {
+  PGB_REQUIRE(nd == 2 || nd == 3, PGB_ERR_INVALID, "%s: ndim must be 2 or 3", who);
+  PGB_REQUIRE(grid != nullptr, PGB_ERR_INVALID, "%s: null grid shape", who);
+  s.nd = nd;
+  const int o = 3 - nd;
+  for (int d = 0; d < 3; ++d) {
+    s.g[d] = 1;
+    s.n[d] = 1;
+    s.off[d] = 0;
+  }
+  for (int d = 0; d < nd; ++d) {
+    s.g[o + d] = static_cast<int>(grid[d]);
+    s.n[o + d] = image ? static_cast<int>(image[d]) : static_cast<int>(grid[d]);
+    PGB_REQUIRE(s.g[o + d] >= 1 && s.n[o + d] >= 1 && s.n[o + d] <= s.g[o + d], PGB_ERR_INVALID,
+                "%s: image extent must be within the grid extent", who);
+    s.off[o + d] = (s.g[o + d] - s.n[o + d]) / 2;
+  }
+  return PGB_OK;
+}
+
+}  // namespace pgb
+
+using namespace pgb;
+
+extern "C" {
+
+int pgb_fft_expand(const void* x, const void* smaps, void* u, int64_t B, int64_t C, int ndim,
+                   const int64_t* grid_shape, const int64_t* image_shape, float scale, int x_has_coils,
+                   void* stream) {
+  clear_error();
+  Shape3 s;
+  int st = make_shape(ndim, grid_shape, image_shape, s, "fft_expand");
+  if (st) return st;
+  PGB_REQUIRE(B >= 0 && C >= 1, PGB_ERR_INVALID, "fft_expand: invalid B/C");
+  if (B == 0) return PGB_OK;
+  PGB_REQUIRE(x && u, PGB_ERR_INVALID, "fft_expand: null pointer");
+  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
+  fft_expand_kernel<<<grid_for(B * C * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(x), static_cast<const float2*>(smaps), static_cast<float2*>(u),
+      static_cast<int>(B), static_cast<int>(C), s, scale, x_has_coils);
+  PGB_LAUNCH_CHECK("fft_expand");
+  return PGB_OK;
+}
+
+int pgb_fft_combine(const void* v, const void* smaps, void* out, int64_t B, int64_t C, int ndim,
+                    const int64_t* grid_shape, const int64_t* image_shape, float scale, const void* add,
+                    float add_scale, void* stream) {
+  clear_error();
+  Shape3 s;
+  int st = make_shape(ndim, grid_shape, image_shape, s, "fft_combine");
+  if (st) return st;
+  PGB_REQUIRE(B >= 0 && C >= 1, PGB_ERR_INVALID, "fft_combine: invalid B/C");
+  if (B == 0) return PGB_OK;
+  PGB_REQUIRE(v && out, PGB_ERR_INVALID, "fft_combine: null pointer");
+  const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
+  fft_combine_kernel<<<grid_for(B * (smaps ? 1 : C) * I, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(v), static_cast<const float2*>(smaps), static_cast<float2*>(out),
+      static_cast<int>(B), static_cast<int>(C), s, scale, static_cast<const float2*>(add), add_scale);
+  PGB_LAUNCH_CHECK("fft_combine");
+  return PGB_OK;
+}
+
+int pgb_sparse_scatter(const void* data, const int32_t* cellpos, const float* w, void* u, int64_t BC,
+                       int64_t R, int64_t G, void* stream) {
+  clear_error();
+  PGB_REQUIRE(BC >= 0 && R >= 0 && G >= 0, PGB_ERR_INVALID, "sparse_scatter: negative size");
+  if (BC == 0 || R == 0 || G == 0) return PGB_OK;
+  PGB_REQUIRE(data && cellpos && w && u, PGB_ERR_INVALID, "sparse_scatter: null pointer");
+  sparse_scatter_kernel<<<grid_for(BC * R, 256, 148 * 16), 256, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(data), cellpos, w, static_cast<float2*>(u), static_cast<int>(BC), R, G);
+  PGB_LAUNCH_CHECK("sparse_scatter");
+  return PGB_OK;
+}
+
+int pgb_sparse_gather(const void* U, const int32_t* cellpos, const float* w, void* out, int64_t BC,
+                      int64_t R, int64_t G, void* stream) {
+  clear_error();
+  PGB_REQUIRE(BC >= 0 && R >= 0 && G >= 0, PGB_ERR_INVALID, "sparse_gather: negative size");
+  if (BC == 0 || R == 0) return PGB_OK;
+  PGB_REQUIRE(U && cellpos && w && out, PGB_ERR_INVALID, "sparse_gather: null pointer");
+  sparse_gather_kernel<<<grid_for(BC * R, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(U), cellpos, w, static_cast<float2*>(out), static_cast<int>(BC), R, G);
+  PGB_LAUNCH_CHECK("sparse_gather");
+  return PGB_OK;
+}
+
+int pgb_psf_apply(void* U, const float* psf, int64_t BC, int64_t G, void* stream) {
+  clear_error();
+  PGB_REQUIRE(BC >= 0 && G >= 0, PGB_ERR_INVALID, "psf_apply: negative size");
+  if (BC == 0 || G == 0) return PGB_OK;
+  PGB_REQUIRE(U && psf, PGB_ERR_INVALID, "psf_apply: null pointer");
+  psf_apply_kernel<<<grid_for(BC * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(static_cast<float2*>(U),
+                                                                                psf, static_cast<int>(BC), G);
+  PGB_LAUNCH_CHECK("psf_apply");
+  return PGB_OK;
+}
+
+int pgb_fft_shift(const void* src, const float* mask, void* dst, int64_t BC, int ndim,
+                  const int64_t* grid_shape, float scale, int to_centred, void* stream) {
+  clear_error();
+  Shape3 s;
+  int st = make_shape(ndim, grid_shape, nullptr, s, "fft_shift");
+  if (st) return st;
+  PGB_REQUIRE(BC >= 0, PGB_ERR_INVALID, "fft_shift: negative size");
+  if (BC == 0) return PGB_OK;
+  PGB_REQUIRE(src && dst && src != dst, PGB_ERR_INVALID, "fft_shift: null or aliased pointers");
+  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
+  fft_shift_kernel<<<grid_for(BC * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(src), mask, static_cast<float2*>(dst), static_cast<int>(BC), s, scale,
+      to_centred);
+  PGB_LAUNCH_CHECK("fft_shift");
+  return PGB_OK;
+}
+
+}  // extern "C"

@@ -83,3 +83,47 @@ def test_oracle_l0_primitives_match_reference():
     assert rel_l2(po, z["ref_po"]) < 1e-6
     pb = og.psf_outer_basis(G, z["pb_basis"].shape[0], z["sa_idx"], z["ps_wsq"], z["pb_basis"], z["pb_tix"])
     assert rel_l2(pb, z["ref_pb"]) < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# Cartesian operators (SparseFFT / Toeplitz / MaskedFFT / CG)
+# ---------------------------------------------------------------------------
+from oracle import operators as oo  # noqa: E402
+
+
+def _op_setup(name):
+    z = golden(f"ops_{name}.npz")
+    _, shape, img, osf, C = parse_meta(z["meta"])
+    p = og.create_plan(shape, z["in_coords"], osf, 2, "circle")
+    fp = og.fft_plan(p)
+    idx_nat = fp["indices"][fp["inv_perm"]]
+    sw_nat = fp["sqrt_weights"][fp["inv_perm"]].astype(np.float64)
+    return z, shape, tuple(img), p, idx_nat, sw_nat, C
+
+
+@pytest.mark.parametrize("name", ["op2d", "op3d"])
+def test_oracle_sparse_fft_matches_reference(name):
+    z, shape, img, p, idx, sw, C = _op_setup(name)
+    gs = tuple(p["grid_shape"])
+    sm = z["in_smaps"].astype(np.complex128)
+    b = z["in_b"].astype(np.complex128)
+    assert rel_l2(oo.sparse_adjoint(b, idx, sw, gs, img, sm), z["ref_adjoint"]) < 1e-5
+    assert rel_l2(oo.sparse_forward(z["in_x"], idx, sw, gs, img, sm), z["ref_forward"]) < 1e-5
+    assert rel_l2(oo.sparse_adjoint(b, idx, sw, gs, img), z["ref_adjoint_nosmaps"]) < 1e-5
+    assert rel_l2(oo.sparse_forward(z["in_xc"], idx, sw, gs, img), z["ref_forward_nosmaps"]) < 1e-5
+    pg = oo.psf(idx, sw, gs)
+    np.testing.assert_allclose(pg, z["ref_psf"], rtol=1e-5, atol=1e-6)
+    assert rel_l2(oo.toeplitz_normal(z["in_x"], pg, gs, img, sm), z["ref_normal_toep"]) < 1e-5
+    assert rel_l2(oo.toeplitz_normal(z["in_x"], pg, gs, img, sm), z["ref_normal_notoep"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["op2d", "op3d"])
+def test_oracle_cg_matches_reference(name):
+    z, shape, img, p, idx, sw, C = _op_setup(name)
+    gs = tuple(p["grid_shape"])
+    sm = z["in_smaps"].astype(np.complex128)
+    pg = oo.psf(idx, sw, gs)
+    AHb = oo.sparse_adjoint(z["in_b"].astype(np.complex128), idx, sw, gs, img, sm)
+    x = oo.cg(lambda v: oo.toeplitz_normal(v, pg, gs, img, sm), AHb, damp=1e-3, max_iter=8)
+    # the reference iterates in complex64 with FP32 inner products
+    assert rel_l2(x, z["ref_cg"]) < 1e-4
