@@ -324,6 +324,34 @@ PGB_API int pgb_cg_update_p(void* p, const void* r, int64_t n, void* scalars, vo
 /* y += a x */
 PGB_API int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream);
 
+/* =====================================================================
+ * Allocation-free row inner products.  No counterpart in the reference
+ * (FiRMLAB-Pisa/pygrog has no C entry point of this kind; its solvers call
+ * torch.vdot, _solve/_solvers.py:49-139).
+ *
+ * out[r] = sum_i Re(conj(a[r, i]) b[r, i])   (b NULL: sum_i |a[r, i]|^2),
+ * accumulated in FP64, for `rows` contiguous complex64 vectors of n
+ * elements; out is a device array of `rows` doubles.  Same arithmetic as
+ * pgb_dot_f64 mode 0, one vector per row.
+ *
+ * For callers that must not allocate device memory while they run: code
+ * working inside a fixed, pre-reserved memory budget (a reconstruction
+ * service whose pool is fully handed out), real-time loops where an
+ * allocation may block or fail, and bindings from languages with no access
+ * to a device allocator.  Its scratch (block partials and completion
+ * counters, 151,808 bytes) is a static array inside this library, so
+ * nothing is allocated or freed by the call.
+ *
+ * Limit: rows <= 64; larger rows return PGB_ERR_RANGE with a message.
+ * The first call on each device looks up the scratch address (with that
+ * device current) and caches it; make that first call before any stream
+ * capture.  Every call clears the counters it uses on `stream` before its
+ * kernel runs.  All calls on one device share the one scratch array, so
+ * calls that can overlap on the GPU (different streams without ordering
+ * between them) race and give wrong results: order them on one stream. */
+PGB_API int pgb_dot_f64_noalloc(const void* a, const void* b, int64_t n, int64_t rows, double* out,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

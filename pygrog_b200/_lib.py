@@ -97,6 +97,7 @@ _SIGS = {
     "pgb_cg_update_xr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp],
     "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
+    "pgb_dot_f64_noalloc": [_vp, _vp, _i64, _i64, _vp, _vp],
 }
 _SIZE_FUNCS = {
     "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],

@@ -10,6 +10,8 @@
 // Scalar block (double[kScalars]), device memory owned by the caller:
 //   [0] rz_old   [1] pAp   [2] rr (|r|^2)   [3] r0_norm   [4] rel   [5] done
 //   [6] tol      [7] spare
+#include <mutex>
+
 #include "common.cuh"
 
 namespace pgb {
@@ -207,6 +209,127 @@ int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream) {
   axpy_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, as_stream(stream)>>>(static_cast<float2*>(y),
                                                                       static_cast<const float2*>(x), a, n);
   PGB_LAUNCH_CHECK("axpy");
+  return PGB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of dot_f64: per-row FP64 inner products of
+// `rows` contiguous vectors, with its block partials and completion counters
+// in a fixed file-scope device array instead of caller-supplied scratch.
+// ---------------------------------------------------------------------------
+namespace pgb {
+
+constexpr int kNoAllocMaxRows = 64;
+constexpr int kNoAllocPartials = kNoAllocMaxRows * kRedBlocks;       // doubles
+constexpr int kNoAllocCounterWords = kNoAllocMaxRows / 2;            // doubles holding the counters
+constexpr int kNoAllocWords = kNoAllocPartials + kNoAllocCounterWords;  // 151,808 bytes
+
+static_assert(kNoAllocCounterWords * sizeof(double) >= kNoAllocMaxRows * sizeof(unsigned),
+              "counter words hold one unsigned per row");
+
+// Partials: row r, block k at [r * kRedBlocks + k]; counters: unsigned[64]
+// after the partials.  Only the counters must start at zero; every call
+// clears the ones it uses on its stream before the kernel runs.
+static __device__ __align__(256) double g_dot_rows_scratch[kNoAllocWords];
+
+__global__ void __launch_bounds__(kRedThreads) dot_f64_rows_kernel(const float2* __restrict__ a,
+                                                                   const float2* __restrict__ b, int64_t n,
+                                                                   double* __restrict__ out,
+                                                                   double* __restrict__ scratch) {
+  const int row = blockIdx.y;
+  const float2* ar = a + static_cast<int64_t>(row) * n;
+  const float2* br = b ? b + static_cast<int64_t>(row) * n : nullptr;
+  double acc = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 x = ar[i];
+    if (br) {
+      const float2 y = br[i];
+      acc += static_cast<double>(x.x) * y.x + static_cast<double>(x.y) * y.y;
+    } else {
+      acc += static_cast<double>(x.x) * x.x + static_cast<double>(x.y) * x.y;
+    }
+  }
+  const double s = block_sum(acc);
+  double* part = scratch + static_cast<int64_t>(row) * kRedBlocks;
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + kNoAllocPartials) + row;
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += blockDim.x) t += part[i];
+  t = block_sum(t);
+  if (threadIdx.x == 0) {
+    out[row] = t;
+    *counter = 0u;
+  }
+}
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_dot_rows_scratch on the current device, looked up once
+// per device (with that device current) and cached.
+int noalloc_scratch(double** ptr) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("dot_f64_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+    return PGB_ERR_CUDA;
+  }
+  PGB_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, PGB_ERR_RANGE,
+              "dot_f64_noalloc: device ordinal %d above the supported %d", dev, kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_dot_rows_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("dot_f64_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                cudaGetErrorString(e));
+      return PGB_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *ptr = g_noalloc_ptr[dev];
+  return PGB_OK;
+}
+}  // namespace
+
+}  // namespace pgb
+
+extern "C" {
+
+int pgb_dot_f64_noalloc(const void* a, const void* b, int64_t n, int64_t rows, double* out, void* stream) {
+  clear_error();
+  PGB_REQUIRE(n >= 0 && rows >= 0, PGB_ERR_INVALID, "dot_f64_noalloc: negative size");
+  PGB_REQUIRE(rows <= kNoAllocMaxRows, PGB_ERR_RANGE,
+              "dot_f64_noalloc: rows=%lld exceeds the static scratch maximum of %d rows", (long long)rows,
+              kNoAllocMaxRows);
+  if (rows == 0) return PGB_OK;
+  PGB_REQUIRE(out && (a || n == 0), PGB_ERR_INVALID, "dot_f64_noalloc: null pointer");
+  double* scratch = nullptr;
+  const int st = noalloc_scratch(&scratch);
+  if (st != PGB_OK) return st;
+  cudaStream_t s = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(scratch + kNoAllocPartials, 0, static_cast<size_t>(rows) * sizeof(unsigned), s);
+  if (e != cudaSuccess) {
+    set_error("dot_f64_noalloc: clearing the counters failed: %s", cudaGetErrorString(e));
+    return PGB_ERR_CUDA;
+  }
+  const dim3 grid(grid_for(n, kRedThreads, kRedBlocks), static_cast<unsigned>(rows));
+  dot_f64_rows_kernel<<<grid, kRedThreads, 0, s>>>(static_cast<const float2*>(a),
+                                                   static_cast<const float2*>(b), n, out, scratch);
+  PGB_LAUNCH_CHECK("dot_f64_noalloc");
   return PGB_OK;
 }
 
