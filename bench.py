@@ -263,7 +263,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--table-mode", default=None, choices=["v5", "v3", "smem", "factored", "global"])
+    ap.add_argument("--table-mode", default=None, choices=["v6", "v5", "v3", "smem", "factored", "global"])
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
@@ -342,7 +342,7 @@ def main():
 
     # algorithmic bytes per launch (both directions): samples + per-replica metadata + grid
     alg_bytes = N * C * 8 * B + bp.n_valid * 12 + G * C * 8 * B
-    kname = {"v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(bp.mode, "factored_kernel")
+    kname = {"v6": "v6_kernel", "v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(bp.mode, "factored_kernel")
     dom = f"grog_grid_{kname}" if fwd_ms >= adj_ms else f"grog_degrid_{kname}"
     dom_ms = max(fwd_ms, adj_ms)
     peak, peak_kind = _peaks()

@@ -251,6 +251,56 @@ PGB_API int pgb_grog_degrid_v5(const void* grid, int64_t G, void* out, int64_t N
                                const pgb_brick_plan* primary, const pgb_brick_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);
 
+/* Operator-stationary variants (C <= 16, power-of-two bricks of at most
+ * 4096 cells).  Replaces the per-replica operator application of
+ * calib/_grog.py:1283-1295 fused with the scatter of
+ * operator/_sparse_fft.py:416 (forward) and its adjoint.
+ *
+ * Plan layout (device arrays, built by pygrog_b200.calib.BrickPlan6):
+ *   sd[]        int4 {rep_begin, rep_end, uniq_begin, uniq_end} per sub-chunk,
+ *               grouped per CTA in processing order (CTA c owns entries
+ *               cta_ptr[c] .. cta_ptr[c+1]-1; launch uses n_cta CTAs)
+ *   si[]        int2 {brick, flags}: 1 first sub-chunk of a brick item,
+ *               2 last one (flush), 4 the brick is split over several items
+ *   uniq[]      int32 source sample of every staging slot, ascending inside
+ *               a sub-chunk (at most sub_cap <= 512 slots / replicas each)
+ *   meta[]      int2 {cell | slot << 16, inner | outer << 16} per replica
+ *   w[]         float weight per replica
+ *   zero_bricks bricks the forward writes with zeros first (empty + split)
+ * inner_lc / outer_lc (forward) and inner_h_lc / outer_h_lc (adjoint): the
+ * factors (inner = whole table when n_outer == 1; outer unused then) in
+ * lane-chunk layout, entry (q, j, l, t) = M[q][l*RPL + t][j] with RPL = 2
+ * for even C (else 1) and L = C / RPL; M = inner / outer for the forward,
+ * their conjugate transposes for the adjoint.
+ * Shared memory: pgb_grog_v6_smem_bytes(C, cells, n_inner, n_outer, sub_cap). */
+typedef struct pgb_v6_plan {
+  const int32_t* sd;
+  const int32_t* si;
+  const int32_t* cta_ptr;
+  int32_t n_cta;
+  const int32_t* uniq;
+  const int32_t* meta;
+  const float* w;
+  int32_t sub_cap;
+  int32_t gz, gy, gx;
+  int32_t bz, by, bx;
+  int32_t nbz, nby, nbx;
+  const int32_t* zero_bricks;
+  int32_t n_zero_bricks;
+} pgb_v6_plan;
+
+PGB_API size_t pgb_grog_v6_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer,
+                                      int64_t sub_cap);
+PGB_API int pgb_grog_grid_v6(const void* data, int64_t N, void* grid, int64_t G, const void* inner_lc,
+                             int64_t n_inner, const void* outer_lc, int64_t n_outer, int64_t C, int64_t B,
+                             const pgb_v6_plan* plan, void* stream);
+/* primary: every sample at most once (plain stores); secondary (may be NULL):
+ * the remaining replicas (atomic adds); zero_src: samples with no replica. */
+PGB_API int pgb_grog_degrid_v6(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h_lc,
+                               int64_t n_inner, const void* outer_h_lc, int64_t n_outer, int64_t C, int64_t B,
+                               const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
+                               const int32_t* zero_src, int64_t n_zero, void* stream);
+
 /* Replica expansion of interpolate() (calib/_grog.py:668-695):
  * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]
  * data (B,C,N), out (B,C,N*kw); entries outside [0,K) give 0. C <= 32. */

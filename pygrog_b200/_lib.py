@@ -25,6 +25,32 @@ _i32 = ctypes.c_int
 _f32 = ctypes.c_float
 
 
+class V6PlanC(ctypes.Structure):
+    """Mirror of ``pgb_v6_plan``."""
+
+    _fields_ = [
+        ("sd", _vp),
+        ("si", _vp),
+        ("cta_ptr", _vp),
+        ("n_cta", ctypes.c_int32),
+        ("uniq", _vp),
+        ("meta", _vp),
+        ("w", _vp),
+        ("sub_cap", ctypes.c_int32),
+        ("gz", ctypes.c_int32),
+        ("gy", ctypes.c_int32),
+        ("gx", ctypes.c_int32),
+        ("bz", ctypes.c_int32),
+        ("by", ctypes.c_int32),
+        ("bx", ctypes.c_int32),
+        ("nbz", ctypes.c_int32),
+        ("nby", ctypes.c_int32),
+        ("nbx", ctypes.c_int32),
+        ("zero_bricks", _vp),
+        ("n_zero_bricks", ctypes.c_int32),
+    ]
+
+
 class BrickPlanC(ctypes.Structure):
     """Mirror of ``pgb_brick_plan``."""
 
@@ -98,11 +124,14 @@ _SIGS = {
     "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
     "pgb_dot_f64_noalloc": [_vp, _vp, _i64, _i64, _vp, _vp],
+    "pgb_grog_grid_v6": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
+    "pgb_grog_degrid_v6": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
 }
 _SIZE_FUNCS = {
     "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],
     "pgb_grog_v3_smem_bytes": [_i64, _i64, _i64, _i32],
     "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
+    "pgb_grog_v6_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_reduce_scratch_bytes": [],
 }
 

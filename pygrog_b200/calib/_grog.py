@@ -34,6 +34,7 @@ import torch
 
 from .. import _lib
 from ._grappa import KernelTable
+from ._plan6 import BrickPlan6, lane_chunk
 
 _DEFAULT_DEVICE = "cuda"
 
@@ -446,6 +447,10 @@ class GrogGridder:
     """Fused GROG gridding operator for one trajectory: brick plans + tables.
 
     Kernel families (chosen from the shared-memory budget of one CTA):
+      ``"v6"``        C <= 16: operator-stationary slots (outer factor rows
+                      in registers along sorted runs, inner factor or whole
+                      table in shared memory), dynamic work queue;
+      ``"v5"``        C <= 16: one lane per replica;
       ``"v3"``        C <= 16: whole table or its inner factor in shared
                       memory, sub-chunks staged ahead in shared memory by
                       persistent CTAs, adjoint as store pass + atomic pass;
@@ -479,8 +484,26 @@ class GrogGridder:
             cells = br[0] * br[1] * br[2]
             return lib.pgb_grog_v5_smem_bytes(C, cells, n_inner, n_outer) <= _SMEM_V3
 
+        def v6_fits(n_in, n_out, br, sub):
+            cells = br[0] * br[1] * br[2]
+            return lib.pgb_grog_v6_smem_bytes(C, cells, n_in, n_out, sub) <= _SMEM_V3
+
         chosen = None
-        if mode in (None, "v5") and C <= 16:
+        self.sub_cap = None
+        if mode in (None, "v6") and C <= 16:
+            n_out_f = int(factors[0].shape[0]) if factors is not None else None
+            for sub in (128, 96, 64):
+                for br in cand:
+                    if K <= 65535 and v6_fits(K, 1, br, sub):
+                        chosen = ("v6", br, False)
+                    elif n_fact is not None and n_fact <= 65535 and v6_fits(n_fact, n_out_f, br, sub):
+                        chosen = ("v6", br, True)
+                    if chosen is not None:
+                        self.sub_cap = sub
+                        break
+                if chosen is not None:
+                    break
+        if chosen is None and mode in (None, "v5") and C <= 16:
             for br in cand:
                 if v5_fits(K, 1, br) and K <= 16384:
                     chosen = ("v5", br, False)
@@ -498,7 +521,7 @@ class GrogGridder:
                     chosen = ("v3", br, True)
                     break
         if chosen is None:
-            if mode in ("v3", "v5"):
+            if mode in ("v3", "v5", "v6"):
                 raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
             br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
                 (4, 8, 8) if ndim == 3 else (1, 16, 16))
@@ -527,11 +550,23 @@ class GrogGridder:
             self.inner = torch.as_tensor(table).to(dev).contiguous()
             self.inner_h = self.inner.conj().transpose(-1, -2).contiguous()
             self.outer = self.outer_h = None
+        self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6)
+        if self.mode == "v6":
+            self.inner_lc = lane_chunk(self.inner)
+            self.inner_h_lc = lane_chunk(self.inner_h)
+            self.outer_lc = lane_chunk(self.outer) if self.outer is not None else None
+            self.outer_h_lc = lane_chunk(self.outer_h) if self.outer_h is not None else None
+            kw6 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap)
+            self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, **kw6)
+            first = _first_valid_mask(target_idx, kw)
+            self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kw6)
+            if self.plan.n_valid > self.adj_plan.n_valid:
+                self.plan2 = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kw6)
+            return
         pack = "split" if self.mode in ("v3", "v5") else "wide"
         kwargs = dict(brick=brick, chunk=chunk, n_outer=self.n_outer, pack=pack,
                       order="inner" if self.mode == "v5" else "cell")
         self.plan = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, **kwargs)
-        self.plan2 = None  # adjoint secondary replicas (v3 / v5)
         self.adj_plan = self.plan
         if self.mode in ("v3", "v5"):
             first = _first_valid_mask(target_idx, kw)
@@ -546,9 +581,11 @@ class GrogGridder:
     def launches_per_call(self, adjoint: bool) -> int:
         bp = self.plan
         if adjoint:
-            if self.mode in ("v3", "v5"):
+            if self.mode in ("v3", "v5", "v6"):
                 return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
             return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
+        if self.mode == "v6":
+            return 1 + (1 if bp.zero_bricks.numel() else 0)
         return 1 + (1 if bp.split_bricks.numel() else 0)
 
     def _outer_ptr(self, h: bool):
@@ -561,7 +598,11 @@ class GrogGridder:
         G = out.shape[-1]
         bp = self.plan
         st = _lib.stream_ptr(data.device)
-        if self.mode == "global":
+        if self.mode == "v6":
+            olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
+            _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
+                      self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
+        elif self.mode == "global":
             _lib.call("pgb_grog_grid", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
                       self.inner.shape[0], C, B, _ctypes_ref(bp._c_all), st)
         else:
@@ -577,7 +618,13 @@ class GrogGridder:
         bp = self.adj_plan
         st = _lib.stream_ptr(grid.device)
         zs = bp.zero_src.data_ptr() if bp.zero_src.numel() else None
-        if self.mode in ("v3", "v5"):
+        if self.mode == "v6":
+            sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
+            olc = self.outer_h_lc.data_ptr() if self.outer_h_lc is not None else None
+            _lib.call("pgb_grog_degrid_v6", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h_lc.data_ptr(),
+                      self.inner_h.shape[0], olc, self.n_outer, C, B,
+                      _ctypes_ref(bp._c), sec, zs, int(bp.zero_src.numel()), st)
+        elif self.mode in ("v3", "v5"):
             sec = _ctypes_ref(self.plan2._c_nonempty) if self.plan2 is not None else None
             _lib.call("pgb_grog_degrid_v3" if self.mode == "v3" else "pgb_grog_degrid_v5", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
                       self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,

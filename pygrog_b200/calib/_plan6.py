@@ -1,0 +1,210 @@
+"""Replica plan of the operator-stationary gridding kernels (``csrc/grog_v6.cu``).
+
+The reference applies ``T[e]`` to every replica of every sample
+(``calib/_grog.py:1283-1295``) and then scatters the replicas into the grid
+(``operator/_sparse_fft.py:416``).  The fused kernels need the valid
+replicas grouped by grid brick and, inside a brick, cut into sub-chunks of
+at most ``sub_cap`` replicas along the sample index; inside a sub-chunk the
+replicas are ordered by (outer table index, inner table index, cell) so a
+slot of lanes can keep the outer factor's rows in registers along a run.
+Everything here is integer bookkeeping done once per trajectory on the GPU
+with torch sorts; the kernels only read the result.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import _lib
+
+
+def lane_chunk(table: torch.Tensor) -> torch.Tensor:
+    """``(K, C, C)`` row-major operators -> lane-chunk layout ``(K, C, L, RPL)``.
+
+    Entry ``[q, j, l, t] = M[q][l * RPL + t][j]`` with ``RPL = 2`` for even
+    ``C`` (else 1) and ``L = C // RPL``: lane ``l`` of a slot reads the RPL
+    entries of column ``j`` it needs as one contiguous word.
+    """
+    K, C, _ = table.shape
+    rpl = 2 if C % 2 == 0 else 1
+    L = C // rpl
+    return table.reshape(K, L, rpl, C).permute(0, 3, 1, 2).contiguous()
+
+
+class BrickPlan6:
+    """Valid replicas in sub-chunk order with per-replica ``(cell, slot, inner, outer)``.
+
+    Arrays (all on the plan's device unless noted):
+      ``subs``   int32 (n_subs, 4) ``{rep_begin, rep_end, uniq_begin, uniq_end}``
+      ``uniq``   int32 source sample of every staging slot
+      ``meta``   int32 (n_valid, 2) ``{cell | slot << 16, inner | outer << 16}``
+      ``w``      float32 replica weight
+      ``sd`` / ``si`` / ``cta_ptr``  per-CTA sub-chunk streams: descriptor,
+                 ``{brick, flags}`` (1 first of item, 2 last, 4 split brick)
+      ``work``   (host) int32 (n_items, 5) ``{brick, sub_begin, sub_end, split, cta}``
+      ``zero_bricks`` bricks the forward zeroes first (empty and split)
+      ``zero_src`` samples with no replica in this plan; ``multi`` whether a
+      sample has more than one.
+    """
+
+    def __init__(
+        self,
+        target_idx: torch.Tensor,
+        interp_idx: torch.Tensor,
+        rep_weight: torch.Tensor,
+        kw: int,
+        grid_shape,
+        brick,
+        n_outer: int = 1,
+        mask: torch.Tensor | None = None,
+        sub_cap: int = 256,
+        item_subs: int = 8,
+        n_cta: int | None = None,
+    ):
+        dev = target_idx.device
+        grid_shape = tuple(int(s) for s in grid_shape)
+        if len(grid_shape) == 2:
+            gz, gy, gx = 1, grid_shape[0], grid_shape[1]
+        else:
+            gz, gy, gx = grid_shape
+        bz, by, bx = (int(b) for b in brick)
+        for b in (bz, by, bx):
+            if b < 1 or (b & (b - 1)):
+                raise ValueError("brick extents must be powers of two")
+        self.grid = (gz, gy, gx)
+        self.brick = (bz, by, bx)
+        self.nb = ((gz + bz - 1) // bz, (gy + by - 1) // by, (gx + bx - 1) // bx)
+        self.cells = cells = bz * by * bx
+        if cells > 4096:
+            raise ValueError("brick too large (max 4096 cells)")
+        if not 1 <= sub_cap <= 512:
+            raise ValueError("sub_cap must be in 1..512")
+        self.sub_cap = int(sub_cap)
+        self.n_outer = int(n_outer)
+        n_bricks = self.nb[0] * self.nb[1] * self.nb[2]
+
+        tgt = target_idx.reshape(-1)
+        self.n_src = n_src = tgt.numel() // kw
+        valid = tgt >= 0
+        if mask is not None:
+            valid = valid & mask.reshape(-1)
+        r = torch.nonzero(valid).squeeze(1)
+        t = tgt[r]
+        z = t // (gy * gx)
+        rem = t - z * (gy * gx)
+        y = rem // gx
+        x = rem - y * gx
+        brick_id = ((z // bz) * self.nb[1] + (y // by)) * self.nb[2] + (x // bx)
+        cl = ((z % bz) * by + (y % by)) * bx + (x % bx)
+        src = r // kw
+        e = interp_idx.reshape(-1)[r].to(torch.int64)
+        q = e // self.n_outer
+        k = e - q * self.n_outer
+        w = rep_weight.reshape(-1)[r].to(torch.float32)
+        if e.numel() and (int(q.max()) >= 65536 or self.n_outer > 65536):
+            raise ValueError("table factors too large for 16-bit indices")
+
+        # (1) sub-chunks: replicas of a brick in sample order, sub_cap at a time
+        _, p1 = torch.sort(brick_id * n_src + src, stable=True)
+        brick_id, cl, src, q, k, w = (a[p1] for a in (brick_id, cl, src, q, k, w))
+        n = int(brick_id.numel())
+        cnt = torch.bincount(brick_id, minlength=n_bricks)
+        start = torch.cumsum(cnt, 0) - cnt
+        pos = torch.arange(n, device=dev) - start[brick_id]
+        nsub_b = (cnt + self.sub_cap - 1) // self.sub_cap
+        sub_first = torch.cumsum(nsub_b, 0) - nsub_b
+        sub_id = sub_first[brick_id] + pos // self.sub_cap
+        n_subs = int(nsub_b.sum())
+        # staging slots: distinct samples of a sub-chunk, ascending
+        uk, inv = torch.unique_consecutive(sub_id * n_src + src, return_inverse=True)
+        uniq_sub = uk // n_src
+        ucnt = torch.bincount(uniq_sub, minlength=n_subs)
+        ubeg = torch.cumsum(ucnt, 0) - ucnt
+        slot = inv - ubeg[sub_id]
+
+        # (2) order inside a sub-chunk: (outer, inner, cell)
+        n_in = int(q.max()) + 1 if n else 1
+        key2 = ((sub_id * self.n_outer + k) * n_in + q) * cells + cl
+        _, p2 = torch.sort(key2, stable=True)
+        sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
+        self.meta = torch.stack([cl | (slot << 16), q | (k << 16)], dim=1).to(torch.int32).contiguous()
+        self.w = w.contiguous()
+        self.uniq = (uk - uniq_sub * n_src).to(torch.int32).contiguous()
+        rcnt = torch.bincount(sub_id, minlength=n_subs)
+        rbeg = torch.cumsum(rcnt, 0) - rcnt
+        self.subs = torch.stack([rbeg, rbeg + rcnt, ubeg, ubeg + ucnt], dim=1).to(torch.int32).contiguous()
+        self.n_valid = n
+        self.n_subs = n_subs
+        self.rep_src = src.to(torch.int32)  # replica -> sample, in kernel order (host checks)
+
+        # (3) brick items of at most item_subs sub-chunks, assigned largest
+        # first to the least loaded CTA; each CTA gets a flat sub-chunk stream
+        nit_b = (nsub_b + item_subs - 1) // item_subs
+        brick_rep = torch.repeat_interleave(torch.arange(n_bricks, device=dev), nit_b)
+        first = torch.cumsum(nit_b, 0) - nit_b
+        kk = torch.arange(brick_rep.numel(), device=dev) - first[brick_rep]
+        s0 = sub_first[brick_rep] + kk * item_subs
+        s1 = torch.minimum(s0 + item_subs, sub_first[brick_rep] + nsub_b[brick_rep])
+        split = (nit_b[brick_rep] > 1).to(torch.int64)
+        rcum = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), torch.cumsum(rcnt, 0)])
+        reps = (rcum[s1] - rcum[s0]).cpu().numpy()
+        n_cta = int(n_cta) if n_cta is not None else _sm_count(dev)
+        cta = _lpt_assign(reps + cells // 4, n_cta)
+        order = np.lexsort((-reps, cta))  # per CTA, largest item first
+        items = torch.stack([brick_rep, s0, s1, split], dim=1).cpu().numpy()[order]
+        cta = cta[order]
+        self.work = torch.from_numpy(np.concatenate([items, cta[:, None]], 1).astype(np.int32))
+        nsub_i = items[:, 2] - items[:, 1]
+        ent_item = np.repeat(np.arange(len(items)), nsub_i)
+        ent_first = np.cumsum(nsub_i) - nsub_i
+        sub_idx = items[ent_item, 1] + (np.arange(ent_item.size) - ent_first[ent_item])
+        flags = ((sub_idx == items[ent_item, 1]) * 1 + (sub_idx == items[ent_item, 2] - 1) * 2
+                 + items[ent_item, 3] * 4)
+        sub_idx_t = torch.from_numpy(sub_idx.astype(np.int64)).to(dev)
+        self.sd = self.subs[sub_idx_t].contiguous()
+        self.si = torch.from_numpy(np.stack([items[ent_item, 0], flags], 1).astype(np.int32)).to(dev).contiguous()
+        per_cta = np.bincount(cta[ent_item], minlength=n_cta) if ent_item.size else np.zeros(n_cta, np.int64)
+        self.cta_ptr = torch.from_numpy(np.concatenate([[0], np.cumsum(per_cta)]).astype(np.int32)).to(dev)
+        self.n_cta = n_cta
+        self.cta_cost = np.bincount(cta, weights=reps + cells // 4, minlength=n_cta) if len(cta) else np.zeros(n_cta)
+        split_b = nit_b > 1
+        self.split_bricks = torch.nonzero(split_b).squeeze(1).to(torch.int32).contiguous()
+        self.zero_bricks = torch.nonzero(split_b | (cnt == 0)).squeeze(1).to(torch.int32).contiguous()
+        per_src = torch.bincount(src, minlength=n_src)
+        self.multi = bool(int(per_src.max()) > 1) if per_src.numel() else False
+        self.zero_src = torch.nonzero(per_src == 0).squeeze(1).to(torch.int32).contiguous()
+        self._c = self._struct()
+
+    def _struct(self) -> _lib.V6PlanC:
+        gz, gy, gx = self.grid
+        bz, by, bx = self.brick
+        nbz, nby, nbx = self.nb
+
+        def ptr(t):
+            return t.data_ptr() if t.numel() else None
+
+        return _lib.V6PlanC(
+            ptr(self.sd), ptr(self.si), self.cta_ptr.data_ptr(), self.n_cta if self.sd.numel() else 0,
+            ptr(self.uniq), ptr(self.meta), ptr(self.w), self.sub_cap, gz, gy, gx, bz, by, bx, nbz, nby, nbx,
+            ptr(self.zero_bricks), int(self.zero_bricks.numel()),
+        )
+
+
+def _sm_count(dev) -> int:
+    if dev.type == "cuda":
+        return int(torch.cuda.get_device_properties(dev).multi_processor_count)
+    return 148
+
+
+def _lpt_assign(cost: np.ndarray, n_bins: int) -> np.ndarray:
+    """Longest-processing-time-first assignment of items to ``n_bins`` bins."""
+    import heapq
+
+    out = np.zeros(len(cost), dtype=np.int64)
+    heap = [(0.0, b) for b in range(n_bins)]
+    for i in np.argsort(-cost, kind="stable"):
+        load, b = heapq.heappop(heap)
+        out[i] = b
+        heapq.heappush(heap, (load + float(cost[i]), b))
+    return out

@@ -124,3 +124,89 @@ def test_brick_plan_split_packing_and_first_valid_mask():
     for n in range(0, 2000, 37):
         if valid[n].any():
             assert first[n, np.argmax(valid[n])]
+
+
+@pytest.mark.parametrize("shape,brick,n_outer,sub_cap", [
+    ((40, 70), (1, 16, 32), 11, 64),
+    ((20, 17, 33), (4, 8, 8), 11, 32),
+    ((24, 16, 40), (8, 8, 8), 1, 256),
+])
+def test_brick_plan6_invariants(shape, brick, n_outer, sub_cap):
+    from pygrog_b200.calib._plan6 import BrickPlan6, lane_chunk
+
+    rng = np.random.default_rng(5)
+    kw = 3
+    tgt, _, w = _toy_plan(shape, 3000, kw, rng, hot=1500)
+    idx = torch.from_numpy(rng.integers(0, 11 * 121, size=(3000, kw)).astype(np.int64))
+    n_cta = 7
+    bp = BrickPlan6(tgt, idx, w, kw, shape, brick, n_outer=n_outer, sub_cap=sub_cap, item_subs=4, n_cta=n_cta)
+    t_all = tgt.numpy().reshape(-1)
+    i_all = idx.numpy().reshape(-1)
+    w_all = w.numpy().reshape(-1)
+    r = np.nonzero(t_all >= 0)[0]
+    assert bp.n_valid == r.size
+    subs = bp.subs.numpy()
+    meta = bp.meta.numpy().astype(np.int64)
+    uniq = bp.uniq.numpy()
+    cl = meta[:, 0] & 0xFFFF
+    slot = meta[:, 0] >> 16
+    q = meta[:, 1] & 0xFFFF
+    k = meta[:, 1] >> 16
+    # sub-chunks tile the replica list and the slot list in order
+    assert subs[0, 0] == 0 and subs[-1, 1] == bp.n_valid and np.all(subs[1:, 0] == subs[:-1, 1])
+    assert subs[0, 2] == 0 and subs[-1, 3] == uniq.size and np.all(subs[1:, 2] == subs[:-1, 3])
+    assert np.all(subs[:, 1] - subs[:, 0] <= sub_cap) and np.all(subs[:, 1] > subs[:, 0])
+    # per-CTA streams: every sub-chunk exactly once, items contiguous with first/last flags
+    sd = bp.sd.numpy()
+    si = bp.si.numpy()
+    ptr = bp.cta_ptr.numpy()
+    assert ptr[0] == 0 and ptr[-1] == len(subs) and len(ptr) == n_cta + 1
+    seen = sorted(map(tuple, sd.tolist()))
+    assert seen == sorted(map(tuple, subs.tolist()))
+    brick_of_sub = {}
+    for c in range(n_cta):
+        ent = si[ptr[c]:ptr[c + 1]]
+        if len(ent) == 0:
+            continue
+        assert ent[0, 1] & 1 and ent[-1, 1] & 2  # stream starts and ends on item boundaries
+        for j in range(len(ent)):
+            if j and not ent[j, 1] & 1:
+                assert ent[j, 0] == ent[j - 1, 0] and not ent[j - 1, 1] & 2
+        for row, e in zip(sd[ptr[c]:ptr[c + 1]], ent):
+            brick_of_sub[tuple(row)] = int(e[0])
+    work = bp.work.numpy()
+    split_bricks = set(bp.split_bricks.numpy().tolist())
+    for b, s0, s1, split, c in work:
+        assert 1 <= s1 - s0 <= 4 and split == (b in split_bricks)
+    nb = int(np.prod(bp.nb))
+    occupied = set(work[:, 0].tolist())
+    assert set(bp.zero_bricks.numpy().tolist()) == (set(range(nb)) - occupied) | split_bricks
+    # LPT keeps the CTAs balanced
+    cost = bp.cta_cost
+    assert cost.max() <= cost.mean() * 1.5 + (work[:, 2] - work[:, 1]).max() * sub_cap
+    gz, gy, gx = bp.grid
+    bz, by, bx = bp.brick
+    nby, nbx = bp.nb[1], bp.nb[2]
+    triples = []
+    for s, (r0, r1, u0, u1) in enumerate(subs):
+        us = uniq[u0:u1]
+        assert np.all(np.diff(us) > 0)  # staged samples ascending and distinct
+        assert np.all(slot[r0:r1] < u1 - u0)
+        key = (k[r0:r1] * 65536 + q[r0:r1]) * bp.cells + cl[r0:r1]
+        assert np.all(np.diff(key) >= 0)  # (outer, inner, cell) order
+        b = brick_of_sub[(r0, r1, u0, u1)]
+        biz, biy, bix = b // (nby * nbx), (b // nbx) % nby, b % nbx
+        c = cl[r0:r1]
+        cell = ((biz * bz + c // (by * bx)) * gy + biy * by + (c // bx) % by) * gx + bix * bx + c % bx
+        for j in range(r1 - r0):
+            triples.append((int(us[slot[r0 + j]]), int(cell[j]), int(q[r0 + j] * n_outer + k[r0 + j]),
+                            float(bp.w[r0 + j])))
+    exp = sorted(zip((r // kw).tolist(), t_all[r].tolist(), i_all[r].tolist(), w_all[r].tolist()))
+    assert sorted(triples) == exp
+    # lane-chunk layout: [q, j, l, t] = M[q][l * RPL + t][j]
+    M = torch.randn(5, 12, 12, dtype=torch.complex64)
+    lc = lane_chunk(M)
+    assert lc.shape == (5, 12, 6, 2)
+    assert lc[3, 7, 4, 1] == M[3, 4 * 2 + 1, 7]
+    lc5 = lane_chunk(torch.randn(2, 5, 5, dtype=torch.complex64))
+    assert lc5.shape == (2, 5, 5, 1)
