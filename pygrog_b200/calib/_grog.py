@@ -748,7 +748,20 @@ class GrogInterpolator:
         src_dev = t.device
         if not t.is_complex():
             t = t.to(torch.complex64)
+        if t.device.type == "cpu" and t.is_pinned():
+            # page-locked input: DMA straight from the caller's buffer
+            return t.to(self.device, non_blocking=True), is_numpy, src_dev
         return t.to(self.device), is_numpy, src_dev
+
+    @staticmethod
+    def _to_host(res: torch.Tensor, is_numpy: bool, src_dev):
+        """Return a result to the caller's device; host results land in page-locked memory."""
+        if not is_numpy and src_dev.type != "cpu":
+            return res.to(src_dev)
+        host = torch.empty(res.shape, dtype=res.dtype, pin_memory=True)
+        host.copy_(res, non_blocking=True)
+        torch.cuda.current_stream(res.device).synchronize()
+        return host.numpy() if is_numpy else host
 
     def _check_c64(self, t):
         if t.dtype != torch.complex64:
@@ -820,8 +833,8 @@ class GrogInterpolator:
                     stack_shape=mplan.stack_shape, mask=mplan.mask.cpu().numpy(),
                     density=mplan.density.cpu().numpy(),
                 )
-                return kgrid.cpu().numpy(), npplan
-            return kgrid.to(src_dev), mplan
+                return self._to_host(kgrid, True, src_dev), npplan
+            return self._to_host(kgrid, False, src_dev), mplan
         sparse = self._sparse_flat(t)
         if ret_image:
             from ..operator._sparse_fft import SparseFFT
@@ -834,7 +847,7 @@ class GrogInterpolator:
             ax = img.ndim - len(plan.image_shape) - 1
             image = img.abs().square().sum(ax).sqrt()
             return image.cpu().numpy() if is_numpy else image.to(src_dev)
-        return sparse.cpu().numpy() if is_numpy else sparse.to(src_dev)
+        return self._to_host(sparse, is_numpy, src_dev)
 
     def __call__(self, data, shot_index=None, ret_image=False, grid=False):
         return self.interpolate(data, shot_index, ret_image, grid)
@@ -928,7 +941,7 @@ class GrogInterpolator:
             if S > 1:
                 out[:, s] = o
         res = out.reshape(*batch, *s_shape, C, *plan.grid_shape)
-        return res.cpu().numpy() if is_numpy else res.to(src_dev)
+        return self._to_host(res, is_numpy, src_dev)
 
     def degrid(self, kgrid):
         """Adjoint of :meth:`grid` / ``interpolate(grid=True)`` with respect to ``data``.
@@ -964,7 +977,7 @@ class GrogInterpolator:
             if S > 1:
                 out[:, s] = o
         res = out.reshape(*batch, *s_shape, C, *spatial)
-        return res.cpu().numpy() if is_numpy else res.to(src_dev)
+        return self._to_host(res, is_numpy, src_dev)
 
     # -- shot-by-shot ---------------------------------------------------------------
     def _grid_shot(self, data: torch.Tensor, shot_index: tuple) -> torch.Tensor:

@@ -114,7 +114,8 @@ class BrickPlan6:
         pos = torch.arange(n, device=dev) - start[brick_id]
         nsub_b = (cnt + self.sub_cap - 1) // self.sub_cap
         sub_first = torch.cumsum(nsub_b, 0) - nsub_b
-        sub_id = sub_first[brick_id] + pos // self.sub_cap
+        # near-equal sub-chunks inside a brick keep consecutive sub-chunks balanced
+        sub_id = sub_first[brick_id] + (pos * nsub_b[brick_id]) // torch.clamp(cnt[brick_id], min=1)
         n_subs = int(nsub_b.sum())
         # staging slots: distinct samples of a sub-chunk, ascending
         uk, inv = torch.unique_consecutive(sub_id * n_src + src, return_inverse=True)
