@@ -254,6 +254,87 @@ def run_reference_arm(args):
     return 0
 
 
+def run_serving(dev, seconds: float, rate: float = 200.0, seed: int = 1004) -> dict:
+    """Served GROG + CG-SENSE mix (c0, c2 and two c3 slices) on this GPU.
+
+    Closed-loop capacity (all requests queued at t=0) of the batched server
+    (8 frames per batch, 4 streams) and of the plain single-instance path
+    (one request at a time, one stream), then an open loop of Poisson arrivals
+    at ``rate`` per second for ``seconds`` with p50 / p95 / p99 latency."""
+    import torch
+
+    from pygrog_b200.serve import ReconProtocol, ReconServer, Request, poisson_arrivals
+    from pygrog_b200.workloads import serving_protocols
+
+    specs = serving_protocols(seed)
+    protos = {}
+    for sp in specs:
+        kw = dict(sp)
+        name = kw.pop("name")
+        protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
+                                     device=dev, **kw)
+    names = list(protos)
+    rng = np.random.default_rng(seed)
+
+    def make(n, arrivals=None):
+        out = []
+        for i in range(n):
+            p = protos[names[int(rng.integers(len(names)))]]
+            d = (torch.randn(p.data_shape, dtype=torch.complex64)).pin_memory()
+            out.append(Request(i, p.name, float(arrivals[i]) if arrivals is not None else 0.0, d))
+        return out
+
+    n_closed = 400
+    single = ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=1, device=dev)
+    rep_single = single.run(make(n_closed), realtime=False)
+    del single
+    batched = ReconServer(protos, mem_budget=150 << 30, max_batch=8, n_slots=4, device=dev)
+    rep_batched = batched.run(make(n_closed), realtime=False)
+    arr = poisson_arrivals(rate, seconds, rng)
+    rep_open = batched.run(make(len(arr), arr), realtime=True)
+    return {
+        "mix": {k: {"coils": p.C, "image": list(p.image_shape), "cg_iters": p.max_iter,
+                     "samples": int(np.prod(p.spatial))} for k, p in protos.items()},
+        "memory_budget_gb": 150,
+        "closed_loop_recons_per_s": rep_batched["recons_per_s"],
+        "single_instance_recons_per_s": rep_single["recons_per_s"],
+        "batched_over_single": rep_batched["recons_per_s"] / rep_single["recons_per_s"],
+        "open_loop": {"rate_per_s": rate, "seconds": seconds, **{k: rep_open[k] for k in
+                      ("requests", "recons_per_s", "p50_ms", "p95_ms", "p99_ms", "mean_batch")}},
+        "precision": "complex64 operators, FP64 CG scalars",
+    }
+
+
+def cg_sense_c2(dev, iters: int = 30) -> dict:
+    """Time per CG-SENSE iteration of config c2 (spiral 320^2, 16 coils, Toeplitz on 640^2),
+    one CUDA graph of ``iters`` iterations, CUDA events."""
+    import torch
+
+    from pygrog_b200.serve import ReconProtocol
+    from pygrog_b200.workloads import serving_protocols
+
+    sp = dict(serving_protocols()[1])
+    name = sp.pop("name")
+    p = ReconProtocol(name, sp.pop("shape"), sp.pop("coords"), sp.pop("acr"), sp.pop("smaps"), device=dev, **sp)
+    p.prepare(1, 1, graphs=True)
+    d = torch.randn((1, *p.data_shape), dtype=torch.complex64, device=dev)
+    for _ in range(3):
+        p.recon(d, 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    reps = 5
+    for _ in range(reps):
+        p.recon(d, 0)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    G = int(np.prod(p.op.grid_shape))
+    return {"ms_per_recon": ms, "cg_iters": p.max_iter, "coils": p.C, "grid": list(p.op.grid_shape),
+            "fft_gflop_per_iter": 2 * p.C * 5 * G * float(np.log2(G)) / 1e9,
+            "note": "recon = GROG interpolate + SparseFFT adjoint + graph-replayed CG (Toeplitz normal)"}
+
+
 def main():
     global N_SPOKES, N_READOUT, GRID_N
     ap = argparse.ArgumentParser()
@@ -267,6 +348,7 @@ def main():
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="open-loop serving duration (0: skip)")
     args = ap.parse_args()
     resized = (args.spokes, args.readout, args.grid) != (N_SPOKES, N_READOUT, GRID_N)
     N_SPOKES, N_READOUT, GRID_N = args.spokes, args.readout, args.grid
@@ -374,6 +456,14 @@ def main():
             "api": "GrogInterpolator.grid(pinned host tensor) + GrogInterpolator.degrid(host tensor)",
         }
 
+    serving = cg2 = None
+    if ws == 1 and args.serve_seconds > 0 and not resized:
+        try:
+            cg2 = cg_sense_c2(dev)
+            serving = run_serving(dev, args.serve_seconds)
+        except Exception as exc:  # noqa: BLE001
+            serving = {"error": f"{type(exc).__name__}: {exc}"}
+
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
@@ -415,6 +505,8 @@ def main():
             "gpu_launches": n_launch * args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "cg_sense_c2": cg2,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

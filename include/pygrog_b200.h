@@ -371,6 +371,18 @@ PGB_API int pgb_cg_update_xr(void* x, void* r, const void* p, const void* Ap, in
 /* beta = rr / (rz_old + 1e-30); p = r + beta p; rz_old = rr */
 PGB_API int pgb_cg_update_p(void* p, const void* r, int64_t n, void* scalars, void* scratch,
                             void* stream);
+/* Frame-batched forms of the three CG kernels for `frames` independent
+ * systems solved together (_solve/_solvers.py:49-139 run once per frame):
+ * vectors are (frames, n) contiguous, scalars (frames, 8) doubles with the
+ * layout above, scratch frames * pgb_reduce_scratch_bytes() bytes
+ * (zero-initialised once).  Each frame keeps its own alpha, beta, residual
+ * and done flag. */
+PGB_API int pgb_dot_f64_batched(const void* a, const void* b, int64_t n, int64_t frames, void* scratch,
+                                void* scalars, int out_slot, int mode, void* stream);
+PGB_API int pgb_cg_update_xr_batched(void* x, void* r, const void* p, const void* Ap, int64_t n,
+                                     int64_t frames, const void* scalars, void* stream);
+PGB_API int pgb_cg_update_p_batched(void* p, const void* r, int64_t n, int64_t frames, void* scalars,
+                                    void* scratch, void* stream);
 /* y += a x */
 PGB_API int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream);
 

@@ -16,7 +16,7 @@ reference recurrence with torch tensors (inner products in FP64).
 
 from __future__ import annotations
 
-__all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG"]
+__all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG", "BatchedDeviceCG"]
 
 from collections.abc import Callable
 from typing import Any
@@ -109,6 +109,85 @@ class DeviceCG:
                     callback(k, self.x, rel)
                 if self.scal[5].item() != 0.0:
                     break
+        return self.x
+
+
+class BatchedDeviceCG:
+    """Independent CG solves of up to ``frames`` systems in lock step: one
+    frame-batched normal operator per iteration and per-frame FP64 scalars
+    (each frame follows the single-frame recurrence of ``DeviceCG``, with its
+    own alpha, beta, residual and done flag).  The buffers persist, so one
+    object serves many batches (``load`` F <= frames right-hand sides, then
+    ``run``); everything is stream-ordered on the current stream."""
+
+    def __init__(self, op, frames: int, single_shape, device, damp: float = 0.0, tol: float = 0.0):
+        self.op = op
+        self.cap = int(frames)
+        self.damp = float(damp)
+        self.tol = float(tol)
+        shape = (self.cap, *tuple(int(s) for s in single_shape))
+        self._x = torch.zeros(shape, dtype=torch.complex64, device=device)
+        self._r = torch.empty_like(self._x)
+        self._p = torch.empty_like(self._x)
+        self._Ap = torch.empty_like(self._x)
+        self.n = int(self._x[0].numel())
+        self.words = (int(_lib.load_library().pgb_reduce_scratch_bytes()) + 7) // 8
+        self.scratch = torch.zeros(self.cap * self.words, dtype=torch.float64, device=device)
+        self._scal = torch.zeros(self.cap, 8, dtype=torch.float64, device=device)
+        self.F = 0
+        self._graphs: dict = {}
+        self._pool = None
+
+    def load(self, AHb: torch.Tensor):
+        """Start from x = 0 with right-hand sides ``AHb (F, *single)``."""
+        F = int(AHb.shape[0])
+        if not 1 <= F <= self.cap:
+            raise ValueError(f"BatchedDeviceCG: {F} frames, capacity {self.cap}")
+        self.F = F
+        self.x, self.r, self.p, self.Ap = (t[:F] for t in (self._x, self._r, self._p, self._Ap))
+        self.scal = self._scal[:F]
+        st = _lib.stream_ptr(AHb.device)
+        self.x.zero_()
+        self.r.copy_(AHb)
+        self.p.copy_(AHb)
+        self.scal.zero_()
+        self.scal[:, 6] = self.tol
+        _lib.call("pgb_dot_f64_batched", self.r.data_ptr(), None, self.n, F, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 0, 2, st)
+
+    def step(self):
+        st = _lib.stream_ptr(self.p.device)
+        F = self.F
+        self.op._normal_frames_into(self.p, self.Ap, self.damp)
+        _lib.call("pgb_dot_f64_batched", self.p.data_ptr(), self.Ap.data_ptr(), self.n, F,
+                  self.scratch.data_ptr(), self.scal.data_ptr(), 1, 0, st)
+        _lib.call("pgb_cg_update_xr_batched", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
+                  self.Ap.data_ptr(), self.n, F, self.scal.data_ptr(), st)
+        _lib.call("pgb_dot_f64_batched", self.r.data_ptr(), None, self.n, F, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 2, 1, st)
+        _lib.call("pgb_cg_update_p_batched", self.p.data_ptr(), self.r.data_ptr(), self.n, F,
+                  self.scal.data_ptr(), self.scratch.data_ptr(), st)
+
+    def capture(self, frames: int, max_iter: int):
+        """Record ``max_iter`` iterations for ``frames`` frames as one CUDA graph
+        (operator and FFT plans must have run once for this shape already).
+        Graphs of one object share a memory pool: replay them on one stream."""
+        self.load(torch.zeros((frames, *self._x.shape[1:]), dtype=torch.complex64, device=self._x.device))
+        if self._pool is None:
+            self._pool = torch.cuda.graph_pool_handle()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, pool=self._pool):
+            for _ in range(int(max_iter)):
+                self.step()
+        self._graphs[(int(frames), int(max_iter))] = g
+
+    def run(self, max_iter: int) -> torch.Tensor:
+        g = self._graphs.get((self.F, int(max_iter)))
+        if g is not None:
+            g.replay()
+            return self.x
+        for _ in range(int(max_iter)):
+            self.step()
         return self.x
 
 

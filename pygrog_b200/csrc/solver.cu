@@ -43,11 +43,23 @@ __device__ __forceinline__ double block_sum(double v) {
 // mode: 0 plain dot -> out;  1: out = rr and the CG residual check
 // (rel = sqrt(rr) / r0, done |= rel < tol);  2: r0 initialisation
 // (r0 = sqrt(rr) + 1e-30, rz_old = rr).
+// Frame f = blockIdx.y works on a + f*n, b + f*n with its own scalar block
+// scal + f*kScalars and scratch + f*kScratchWords (gridDim.y == 1: one frame).
+constexpr int kScalars = 8;
+constexpr int kScratchWords = kRedBlocks + 2;  // partials + two unsigned counters (one double)
+
 __global__ void __launch_bounds__(kRedThreads) dot_f64_kernel(const float2* __restrict__ a,
                                                               const float2* __restrict__ b, int64_t n,
                                                               double* __restrict__ scratch,
                                                               double* __restrict__ scal, int out_slot,
                                                               int mode) {
+  {
+    const int64_t f = blockIdx.y;
+    a += f * n;
+    if (b) b += f * n;
+    scratch += f * kScratchWords;
+    scal += f * kScalars;
+  }
   if (mode == 1 && scal[S_DONE] != 0.0) return;  // grid-uniform: converged, skip
   double acc = 0.0;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -97,6 +109,14 @@ __global__ void __launch_bounds__(kRedThreads) dot_f64_kernel(const float2* __re
 __global__ void cg_update_xr_kernel(float2* __restrict__ x, float2* __restrict__ r,
                                     const float2* __restrict__ p, const float2* __restrict__ Ap, int64_t n,
                                     const double* __restrict__ scal) {
+  {
+    const int64_t f = blockIdx.y;
+    x += f * n;
+    r += f * n;
+    p += f * n;
+    Ap += f * n;
+    scal += f * kScalars;
+  }
   if (scal[S_DONE] != 0.0) return;
   const float alpha = static_cast<float>(scal[S_RZ] / (scal[S_PAP] + 1e-30));
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -117,6 +137,13 @@ __global__ void cg_update_xr_kernel(float2* __restrict__ x, float2* __restrict__
 // completion counter in scratch).
 __global__ void cg_update_p_kernel(float2* __restrict__ p, const float2* __restrict__ r, int64_t n,
                                    double* __restrict__ scal, double* __restrict__ scratch) {
+  {
+    const int64_t f = blockIdx.y;
+    p += f * n;
+    r += f * n;
+    scal += f * kScalars;
+    scratch += f * kScratchWords;
+  }
   if (scal[S_DONE] != 0.0) return;
   const double rr = scal[S_RR];
   const float beta = static_cast<float>(rr / (scal[S_RZ] + 1e-30));
@@ -160,7 +187,7 @@ using namespace pgb;
 
 extern "C" {
 
-size_t pgb_reduce_scratch_bytes(void) { return kRedBlocks * sizeof(double) + 2 * sizeof(unsigned) + 8; }
+size_t pgb_reduce_scratch_bytes(void) { return kScratchWords * sizeof(double); }
 
 int pgb_dot_f64(const void* a, const void* b, int64_t n, void* scratch, void* scalars, int out_slot, int mode,
                 void* stream) {
@@ -198,6 +225,50 @@ int pgb_cg_update_p(void* p, const void* r, int64_t n, void* scalars, void* scra
       static_cast<float2*>(p), static_cast<const float2*>(r), n, static_cast<double*>(scalars),
       static_cast<double*>(scratch));
   PGB_LAUNCH_CHECK("cg_update_p");
+  return PGB_OK;
+}
+
+int pgb_dot_f64_batched(const void* a, const void* b, int64_t n, int64_t frames, void* scratch, void* scalars,
+                        int out_slot, int mode, void* stream) {
+  clear_error();
+  PGB_REQUIRE(n >= 0 && frames >= 0 && frames <= 65535 && out_slot >= 0 && out_slot < kScalars && mode >= 0 &&
+                  mode <= 2,
+              PGB_ERR_INVALID, "dot_f64_batched: invalid arguments");
+  if (frames == 0) return PGB_OK;
+  PGB_REQUIRE(a && scratch && scalars, PGB_ERR_INVALID, "dot_f64_batched: null pointer");
+  const dim3 grid(grid_for(n, kRedThreads, kRedBlocks), static_cast<unsigned>(frames));
+  dot_f64_kernel<<<grid, kRedThreads, 0, as_stream(stream)>>>(
+      static_cast<const float2*>(a), static_cast<const float2*>(b), n, static_cast<double*>(scratch),
+      static_cast<double*>(scalars), out_slot, mode);
+  PGB_LAUNCH_CHECK("dot_f64_batched");
+  return PGB_OK;
+}
+
+int pgb_cg_update_xr_batched(void* x, void* r, const void* p, const void* Ap, int64_t n, int64_t frames,
+                             const void* scalars, void* stream) {
+  clear_error();
+  PGB_REQUIRE(n >= 0 && frames >= 0 && frames <= 65535, PGB_ERR_INVALID, "cg_update_xr_batched: invalid sizes");
+  if (n == 0 || frames == 0) return PGB_OK;
+  PGB_REQUIRE(x && r && p && Ap && scalars, PGB_ERR_INVALID, "cg_update_xr_batched: null pointer");
+  const dim3 grid(grid_for(n, 256, 148 * 8), static_cast<unsigned>(frames));
+  cg_update_xr_kernel<<<grid, 256, 0, as_stream(stream)>>>(
+      static_cast<float2*>(x), static_cast<float2*>(r), static_cast<const float2*>(p),
+      static_cast<const float2*>(Ap), n, static_cast<const double*>(scalars));
+  PGB_LAUNCH_CHECK("cg_update_xr_batched");
+  return PGB_OK;
+}
+
+int pgb_cg_update_p_batched(void* p, const void* r, int64_t n, int64_t frames, void* scalars, void* scratch,
+                            void* stream) {
+  clear_error();
+  PGB_REQUIRE(n >= 0 && frames >= 0 && frames <= 65535, PGB_ERR_INVALID, "cg_update_p_batched: invalid sizes");
+  if (n == 0 || frames == 0) return PGB_OK;
+  PGB_REQUIRE(p && r && scalars && scratch, PGB_ERR_INVALID, "cg_update_p_batched: null pointer");
+  const dim3 grid(grid_for(n, 256, 148 * 8), static_cast<unsigned>(frames));
+  cg_update_p_kernel<<<grid, 256, 0, as_stream(stream)>>>(static_cast<float2*>(p), static_cast<const float2*>(r),
+                                                          n, static_cast<double*>(scalars),
+                                                          static_cast<double*>(scratch));
+  PGB_LAUNCH_CHECK("cg_update_p_batched");
   return PGB_OK;
 }
 

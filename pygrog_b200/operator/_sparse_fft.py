@@ -279,6 +279,28 @@ class SparseFFT(SolveMixin):
         st.combine(v, self._smaps_d, out, 1, C, st.ortho, add=x if damp else None, add_scale=damp)
         return out
 
+    def _normal_frames_into(self, x: torch.Tensor, out: torch.Tensor, damp: float = 0.0) -> torch.Tensor:
+        """``out[f] = A^H A x[f] + damp * x[f]`` for F independent frames ``x (F, *single)``
+        already on the device (one batched pass; no host synchronisation)."""
+        if self.stack_shape:
+            raise NotImplementedError("frame-batched normal operator covers unstacked operators")
+        if self.toeplitz:
+            if self._toep_op is None:
+                from .._toep import GrogToeplitzOp
+
+                self._toep_op = GrogToeplitzOp(self, device=self._cdev)
+            return self._toep_op._apply_frames(x, 0, out, damp)
+        F = int(x.shape[0])
+        C = self._n_coils(x.shape[1] if x.ndim > len(self.image_shape) + 1 else 1)
+        k = self._forward_core(x, 0, C)
+        st = self._stage
+        a = self._stack_arrays_dev(0)
+        u = torch.zeros(F, C, *st.grid_shape, dtype=torch.complex64, device=x.device)
+        st.scatter(k, a.cellpos, a.w, u, F * C, a.R, st.G)
+        v = st.ifft(u)
+        st.combine(v, self._smaps_d, out, F, C, st.ortho, add=x if damp else None, add_scale=damp)
+        return out
+
     # ------------------------------------------------------------------
     # batch helpers (reference 1050-1149)
     # ------------------------------------------------------------------

@@ -188,3 +188,28 @@ def config3_slices(seed: int = 1003, n_slices: int = 64):
         C = int(rng.integers(8, 33))
         out.append(dict(spokes=sp, readout=ro, grid=g, coils=C))
     return out
+
+
+def serving_protocols(seed: int = 1004, n_slices: int = 2) -> list[dict]:
+    """Protocol specs of the served-recon mix: the c0 and c2 configurations and
+    ``n_slices`` uneven radial slices of c3 (coil maps from seeded Gaussian
+    bumps, ACR = centre 24^2 of the coil k-space of a seeded phantom).
+    Keyword sets for ``pygrog_b200.serve.ReconProtocol``."""
+    out = []
+    w0 = config0()
+    out.append(dict(name="c0", shape=w0.shape, coords=w0.coords, acr=w0.acr, smaps=w0.smaps, oversamp=1.0,
+                    kernel_width=5, kernel_shape="square", precision=2, lamda=1e-2, max_iter=10))
+    w2 = config2()
+    out.append(dict(name="c2", shape=w2.shape, coords=w2.coords, acr=w2.acr, smaps=w2.smaps, oversamp=2.0,
+                    kernel_width=2, kernel_shape="circle", precision=1, lamda=1e-3, max_iter=30))
+    rng = np.random.default_rng(seed)
+    for i, s in enumerate(config3_slices(seed=1003, n_slices=n_slices)):
+        n, C = s["grid"], s["coils"]
+        coords = radial2d(s["spokes"], s["readout"], n / 2.0)
+        img = ellipse_phantom2d(n, rng)
+        maps = gaussian_coils((n, n), C, rng)
+        acr = center_crop(centered_fft(maps * img, axes=(-2, -1)), 24, 2).astype(np.complex64)
+        out.append(dict(name=f"c3s{i}", shape=(n, n), coords=coords, acr=acr, smaps=maps.astype(np.complex64),
+                        oversamp=1.0, kernel_width=2, kernel_shape="circle", precision=1, lamda=1e-2,
+                        max_iter=20))
+    return out
