@@ -343,6 +343,23 @@ PGB_API int pgb_sparse_scatter(const void* data, const int32_t* cellpos, const f
 PGB_API int pgb_sparse_gather(const void* U, const int32_t* cellpos, const float* w, void* out,
                               int64_t BC, int64_t R, int64_t G, void* stream);
 
+/* Low-rank subspace transfers (replace the per-(coil, component) scatter /
+ * gather loops of gadgets/_subspace.py:311-508 and the PSF matvec of
+ * _toep/_sub_toep.py:236-303).  y (B, C, R) natural sample order, u / U
+ * (B, K, C, G) FFT-order grids, basis (K, T) complex64, tidx (R) int32 index
+ * along the encoding axis, cellpos (R) int32 FFT-order cell, w (R) float.
+ *   scatter: u[b,k,c,cell_r] += w_r * basis[k,t_r] * y[b,c,r]
+ *   gather:  y[b,c,r] = w_r * sum_k conj(basis[k,t_r]) * U[b,k,c,cell_r]
+ *   psf_apply_kk (in place): U[b,k,c,g] = sum_k' P[g,k,k'] * U[b,k',c,g],
+ *            P (G, K, K) complex64, K <= 16. */
+PGB_API int pgb_subspace_scatter(const void* y, const int32_t* cellpos, const float* w, const int32_t* tidx,
+                                 const void* basis, void* u, int64_t B, int64_t C, int64_t K, int64_t T,
+                                 int64_t R, int64_t G, void* stream);
+PGB_API int pgb_subspace_gather(const void* U, const int32_t* cellpos, const float* w, const int32_t* tidx,
+                                const void* basis, void* out, int64_t B, int64_t C, int64_t K, int64_t T,
+                                int64_t R, int64_t G, void* stream);
+PGB_API int pgb_psf_apply_kk(void* U, const void* P, int64_t B, int64_t K, int64_t C, int64_t G, void* stream);
+
 /* U[bc, m] *= psf[m] (real PSF in FFT order; Toeplitz normal operator). */
 PGB_API int pgb_psf_apply(void* U, const float* psf, int64_t BC, int64_t G, void* stream);
 

@@ -110,3 +110,54 @@ def cg(normal, AHb, damp=0.0, max_iter=20, tol=0.0):
         p = r + rz_new / (rz + 1e-30) * p
         rz = rz_new
     return x
+
+
+# ---------------------------------------------------------------------------
+# Low-rank subspace operator (gadgets/_subspace.py:311-508, _toep/_sub_toep.py:120-303)
+# ---------------------------------------------------------------------------
+def sub_adjoint(y, idx_nat, sw_nat, tidx, basis, grid_shape, image_shape, smaps):
+    """y (C, R) natural order -> coefficients (K, *img).
+
+    x_k = sum_c conj(S_c) crop(IFFT(scatter(sw^2 * basis[k, t] * y_c))) (pre_w = sw).
+    """
+    K = basis.shape[0]
+    out = np.zeros((K, *image_shape), dtype=np.complex128)
+    for k in range(K):  # pre-weight sw here, sparse_adjoint applies the second sw
+        out[k] = sparse_adjoint(y * sw_nat * basis[k, tidx], idx_nat, sw_nat, grid_shape, image_shape, smaps)
+    return out
+
+
+def sub_forward(x, idx_nat, sw_nat, tidx, basis, grid_shape, image_shape, smaps):
+    """coefficients (K, *img) -> y (C, R): y_c = sw^2 sum_k conj(basis[k, t]) FFT(pad(S_c x_k))[idx]."""
+    K = basis.shape[0]
+    acc = 0
+    for k in range(K):
+        acc = acc + np.conj(basis[k, tidx]) * sparse_forward(x[k], idx_nat, sw_nat, grid_shape, image_shape, smaps)
+    return acc * sw_nat
+
+
+def sub_psf(idx_nat, sw_nat, tidx, basis, grid_shape):
+    """P[g, k, k'] = sum_{i: idx_i = g} sw_i^4 basis[k, t_i] conj(basis[k', t_i]) -> (*grid, K, K)."""
+    K = basis.shape[0]
+    G = int(np.prod(grid_shape))
+    w4 = sw_nat.astype(np.float64) ** 4
+    P = np.zeros((G, K, K), dtype=np.complex128)
+    for k in range(K):
+        for kp in range(K):
+            np.add.at(P[:, k, kp], idx_nat, w4 * basis[k, tidx] * np.conj(basis[kp, tidx]))
+    return P.reshape(*grid_shape, K, K)
+
+
+def sub_toeplitz_normal(x, P, grid_shape, image_shape, smaps):
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    K = x.shape[0]
+    sl = (slice(None), *_slices(grid_shape, image_shape))
+    out = np.zeros_like(x, dtype=np.complex128)
+    for c in range(smaps.shape[0]):
+        pad = np.zeros((K, *grid_shape), dtype=np.complex128)
+        pad[sl] = smaps[c] * x
+        Kk = fftc(pad, axes)
+        mixed = np.einsum("...ab,b...->a...", P, Kk)
+        out += np.conj(smaps[c]) * ifftc(mixed, axes)[sl]
+    return out

@@ -123,6 +123,9 @@ _SIGS = {
     "pgb_cg_update_xr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp],
     "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
+    "pgb_subspace_scatter": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
+    "pgb_subspace_gather": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
+    "pgb_psf_apply_kk": [_vp, _vp, _i64, _i64, _i64, _i64, _vp],
     "pgb_dot_f64_batched": [_vp, _vp, _i64, _i64, _vp, _vp, _i32, _i32, _vp],
     "pgb_cg_update_xr_batched": [_vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_cg_update_p_batched": [_vp, _vp, _i64, _i64, _vp, _vp, _vp],

@@ -199,7 +199,8 @@ def _device_cg_applicable(op, AHb, preconditioner) -> bool:
         and AHb.device.type == "cuda"
         and AHb.dtype == torch.complex64
         and not getattr(op, "stack_shape", ())
-        and AHb.ndim == len(op.image_shape) + (0 if getattr(op, "smaps", None) is not None else 1)
+        and AHb.ndim == getattr(op, "_single_ndim",
+                                len(op.image_shape) + (0 if getattr(op, "smaps", None) is not None else 1))
     )
 
 

@@ -2,5 +2,12 @@
 
 from ._masked_fft import MaskedFFT, MaskedFFTPlan  # noqa: F401
 from ._sparse_fft import SparseFFT, gather, scatter_add  # noqa: F401
+from ._subspace import (  # noqa: F401
+    SubspaceProjection,
+    SubspaceSparseFFT,
+    SubspaceToeplitzOp,
+    with_subspace,
+)
 
-__all__ = ["SparseFFT", "MaskedFFT", "MaskedFFTPlan", "gather", "scatter_add"]
+__all__ = ["SparseFFT", "MaskedFFT", "MaskedFFTPlan", "gather", "scatter_add", "SubspaceProjection",
+           "SubspaceSparseFFT", "SubspaceToeplitzOp", "with_subspace"]

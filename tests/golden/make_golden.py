@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (see ``refimport.py``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [plans] [l0] [operators] [subspace]
 
 Writes ``tests/golden/*.npz``.  Every array stored under ``ref_*`` is an output
 of the reference implementation itself (its Python package plus its C++
@@ -197,14 +197,57 @@ def make_operator_cases(pg, out):
         print("wrote", name)
 
 
+def make_subspace_cases(pg, out):
+    """SubspaceSparseFFT adjoint / forward / normal (Toeplitz and nested) / CG on
+    a 2-D plan whose natural shape (T, 160, kw) carries T = 5 frames on the
+    encoding axis -3 of the sparse layout (C, T, 160, kw)."""
+    import importlib
+
+    gad = importlib.import_module("pygrog.gadgets")
+    rng = np.random.default_rng(2024)
+    shape, img, C, K, T = (20, 20), (20, 20), 3, 2, 5
+    coords = (rng.standard_normal((T, 160, 2)) * 4).astype(np.float32)
+    g = pg.calib.GrogInterpolator(shape=shape, coords=coords, oversamp=2.0, kernel_width=2, image_shape=img)
+    calib = _c(rng, C, 8, 8)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    smaps = (_c(rng, C, *img) * 0.5).astype(np.complex64)
+    q, _ = np.linalg.qr(_c(rng, T, K, dtype=np.complex128))
+    basis = q.T.astype(np.complex64)  # (K, T) orthonormal rows
+    base_t = pg.operator.SparseFFT(plan=g.plan, smaps=torch.from_numpy(smaps), toeplitz=True)
+    base_n = pg.operator.SparseFFT(plan=g.plan, smaps=torch.from_numpy(smaps), toeplitz=False)
+    sub_t = gad.with_subspace(base_t, torch.from_numpy(basis), encoding_axis=-3)
+    sub_n = gad.with_subspace(base_n, torch.from_numpy(basis), encoding_axis=-3)
+    nat = tuple(int(v) for v in base_t.natural_shape)
+    b = torch.from_numpy(_c(rng, C, *nat))
+    xk = torch.from_numpy(_c(rng, K, *img))
+    rec = dict(
+        in_coords=coords, in_calib=calib, in_smaps=smaps, in_basis=basis, in_b=b.numpy(), in_xk=xk.numpy(),
+        meta=np.array([repr(("sub2d", shape, img, 2.0, C, K, T))]),
+        ref_sub_adjoint=sub_t.adjoint(b).numpy(),
+        ref_sub_forward=sub_t.forward(xk).numpy(),
+        ref_sub_normal_toep=sub_t.normal(xk).numpy(),
+        ref_sub_normal_notoep=sub_n.normal(xk).numpy(),
+    )
+    rec["ref_sub_psf"] = sub_t._toep_op.psf.numpy()
+    rec["ref_sub_cg"] = sub_t.solve(b, method="cg", max_iter=6, damp=1e-3, tol=0.0).numpy()
+    np.savez_compressed(out / "sub_sub2d.npz", **rec)
+    print("wrote sub2d")
+
+
 def main():
     pg = refimport.import_reference()
     torch.set_num_threads(4)
     out = HERE
-    make_plan_cases(pg, out)
-    make_fp64_case(pg, out)
-    make_l0_cases(pg, out)
-    make_operator_cases(pg, out)
+    only = set(sys.argv[1:])
+    if not only or "plans" in only:
+        make_plan_cases(pg, out)
+        make_fp64_case(pg, out)
+    if not only or "l0" in only:
+        make_l0_cases(pg, out)
+    if not only or "operators" in only:
+        make_operator_cases(pg, out)
+    if not only or "subspace" in only:
+        make_subspace_cases(pg, out)
 
 
 if __name__ == "__main__":

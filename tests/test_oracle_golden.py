@@ -127,3 +127,35 @@ def test_oracle_cg_matches_reference(name):
     x = oo.cg(lambda v: oo.toeplitz_normal(v, pg, gs, img, sm), AHb, damp=1e-3, max_iter=8)
     # the reference iterates in complex64 with FP32 inner products
     assert rel_l2(x, z["ref_cg"]) < 1e-4
+
+
+def _sub_setup():
+    z = golden("sub_sub2d.npz")
+    _, shape, img, osf, C, K, T = parse_meta(z["meta"])
+    p = og.create_plan(shape, z["in_coords"], osf, 2, "circle")
+    fp = og.fft_plan(p)
+    idx = fp["indices"][fp["inv_perm"]]
+    sw = fp["sqrt_weights"][fp["inv_perm"]].astype(np.float64)
+    nat = z["in_b"].shape[1:]
+    tidx = np.broadcast_to(np.arange(T).reshape(T, 1, 1), nat).reshape(-1)
+    return z, tuple(p["grid_shape"]), tuple(img), idx, sw, tidx
+
+
+def test_oracle_subspace_matches_reference():
+    z, gs, img, idx, sw, tidx = _sub_setup()
+    sm = z["in_smaps"].astype(np.complex128)
+    B = z["in_basis"].astype(np.complex128)
+    C = sm.shape[0]
+    b = z["in_b"].reshape(C, -1).astype(np.complex128)
+    assert rel_l2(oo.sub_adjoint(b, idx, sw, tidx, B, gs, img, sm), z["ref_sub_adjoint"]) < 1e-5
+    y = oo.sub_forward(z["in_xk"].astype(np.complex128), idx, sw, tidx, B, gs, img, sm)
+    assert rel_l2(y, z["ref_sub_forward"].reshape(C, -1)) < 1e-5
+    P = oo.sub_psf(idx, sw, tidx, B, gs)
+    assert rel_l2(P, z["ref_sub_psf"]) < 1e-5
+    xk = z["in_xk"].astype(np.complex128)
+    assert rel_l2(oo.sub_toeplitz_normal(xk, P, gs, img, sm), z["ref_sub_normal_toep"]) < 1e-5
+    nested = oo.sub_adjoint(oo.sub_forward(xk, idx, sw, tidx, B, gs, img, sm), idx, sw, tidx, B, gs, img, sm)
+    assert rel_l2(nested, z["ref_sub_normal_notoep"]) < 1e-5
+    AHb = oo.sub_adjoint(b, idx, sw, tidx, B, gs, img, sm)
+    x = oo.cg(lambda v: oo.sub_toeplitz_normal(v, P, gs, img, sm), AHb, damp=1e-3, max_iter=6)
+    assert rel_l2(x, z["ref_sub_cg"]) < 1e-4
