@@ -264,9 +264,9 @@ def run_serving(dev, seconds: float, rate: float = 200.0, seed: int = 1004) -> d
     import torch
 
     from pygrog_b200.serve import ReconProtocol, ReconServer, Request, poisson_arrivals
-    from pygrog_b200.workloads import serving_protocols
+    from pygrog_b200.workloads import serving_protocols, subspace_protocol
 
-    specs = serving_protocols(seed)
+    specs = serving_protocols(seed) + [subspace_protocol()]
     protos = {}
     for sp in specs:
         kw = dict(sp)
@@ -274,12 +274,15 @@ def run_serving(dev, seconds: float, rate: float = 200.0, seed: int = 1004) -> d
         protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
                                      device=dev, **kw)
     names = list(protos)
+    # 20% of the requests use the rank-4 subspace protocol, the rest spread evenly
+    others = [k for k in names if not protos[k].subspace]
+    prob = np.array([0.2 if protos[k].subspace else 0.8 / len(others) for k in names])
     rng = np.random.default_rng(seed)
 
     def make(n, arrivals=None):
         out = []
         for i in range(n):
-            p = protos[names[int(rng.integers(len(names)))]]
+            p = protos[names[int(rng.choice(len(names), p=prob))]]
             d = (torch.randn(p.data_shape, dtype=torch.complex64)).pin_memory()
             out.append(Request(i, p.name, float(arrivals[i]) if arrivals is not None else 0.0, d))
         return out
@@ -294,7 +297,8 @@ def run_serving(dev, seconds: float, rate: float = 200.0, seed: int = 1004) -> d
     rep_open = batched.run(make(len(arr), arr), realtime=True)
     return {
         "mix": {k: {"coils": p.C, "image": list(p.image_shape), "cg_iters": p.max_iter,
-                     "samples": int(np.prod(p.spatial))} for k, p in protos.items()},
+                     "samples": int(np.prod(p.spatial)), "share": float(prob[i])}
+                for i, (k, p) in enumerate(protos.items())},
         "memory_budget_gb": 150,
         "closed_loop_recons_per_s": rep_batched["recons_per_s"],
         "single_instance_recons_per_s": rep_single["recons_per_s"],

@@ -217,6 +217,16 @@ class SubspaceSparseFFT(SolveMixin):
             return self._toeplitz()(coeffs)
         return self.adjoint(self.forward(coeffs))
 
+    def _normal_frames_into(self, x: torch.Tensor, out: torch.Tensor, damp: float = 0.0) -> torch.Tensor:
+        """``out[f] = A^H A x[f] + damp x[f]`` for frames ``x (F, K, *image)`` on the device."""
+        if self.stack_shape:
+            raise NotImplementedError("frame-batched normal operator covers unstacked operators")
+        if self.toeplitz:
+            return self._toeplitz()._apply_frames(x, 0, out, damp)
+        y = self._adjoint_core(self._forward_core(x, 0), 0)
+        torch.add(y, x, alpha=damp, out=out) if damp else out.copy_(y)
+        return out
+
     def _normal_into(self, x: torch.Tensor, out: torch.Tensor, damp: float = 0.0) -> torch.Tensor:
         """``out = A^H A x + damp x`` for one frame ``(K, *image)`` on the device."""
         if self.stack_shape:

@@ -37,7 +37,7 @@ import torch
 
 from ._solve import BatchedDeviceCG
 from .calib import GrogInterpolator
-from .operator import SparseFFT
+from .operator import SparseFFT, with_subspace
 
 
 @dataclasses.dataclass
@@ -62,18 +62,26 @@ class ReconProtocol:
 
     def __init__(self, name: str, shape, coords, acr, smaps, *, oversamp=None, kernel_width: int = 2,
                  kernel_shape: str = "circle", precision: int = 1, lamda: float = 0.01, max_iter: int = 20,
-                 damp: float = 1e-3, device="cuda"):
+                 damp: float = 1e-3, basis=None, encoding_axis: int = -3, device="cuda"):
         self.name = name
         self.device = torch.device(device)
         self.interp = GrogInterpolator(shape=shape, coords=coords, oversamp=oversamp, kernel_width=kernel_width,
                                        kernel_shape=kernel_shape, device=self.device)
         self.interp.calc_interp_table(acr, lamda=lamda, precision=precision)
         sm = torch.as_tensor(smaps).to(self.device, torch.complex64)
-        self.op = SparseFFT(plan=self.interp.plan, smaps=sm, toeplitz=True, device=self.device)
+        base = SparseFFT(plan=self.interp.plan, smaps=sm, toeplitz=True, device=self.device)
+        self.subspace = basis is not None
+        if self.subspace:
+            # low-rank subspace (gadgets/_subspace.py): unknowns are K coefficient images
+            self.op = with_subspace(base, torch.as_tensor(basis), encoding_axis=encoding_axis)
+            self.image_shape = (self.op.K, *tuple(base.image_shape))
+        else:
+            self.op = base
+            self.image_shape = tuple(base.image_shape)
         self.pre_w = self.interp.plan.pre_weights.to(self.device, torch.float32)
+        self.natural_shape = tuple(base.natural_shape)
         self.C = int(sm.shape[0])
         self.spatial = tuple(int(s) for s in np.asarray(coords).shape[:-1])
-        self.image_shape = tuple(self.op.image_shape)
         self.max_iter = int(max_iter)
         self.damp = float(damp)
         self._solvers: dict = {}
@@ -88,7 +96,7 @@ class ReconProtocol:
         FFT buffers, CG vectors)."""
         n_s = int(np.prod(self.spatial))
         n_rep = int(self.interp.plan.n_samples)
-        G = int(np.prod(self.op.grid_shape))
+        G = int(np.prod(self.op.grid_shape)) * (self.op.K if self.subspace else 1)
         img = int(np.prod(self.image_shape))
         return 8 * (self.C * n_s + 3 * self.C * n_rep + 3 * self.C * G + 6 * img)
 
@@ -112,8 +120,10 @@ class ReconProtocol:
     def recon(self, data_dev: torch.Tensor, slot: int, max_iter: int | None = None) -> torch.Tensor:
         """``data_dev (F, C, *spatial)`` on the device -> images ``(F, *image_shape)`` (stream-ordered)."""
         sparse = self.interp.interpolate(data_dev)  # (F, C, n_samples)
-        b = sparse * self.pre_w
-        AHb = self.op.adjoint(b)  # (F, *image_shape)
+        if self.subspace:  # the subspace operator applies the sample weights itself
+            AHb = self.op.adjoint(sparse.reshape(sparse.shape[0], self.C, *self.natural_shape))
+        else:
+            AHb = self.op.adjoint(sparse * self.pre_w)  # (F, *image_shape)
         cg = self._solvers[slot]
         cg.load(AHb)
         return cg.run(self.max_iter if max_iter is None else max_iter)

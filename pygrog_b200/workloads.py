@@ -213,3 +213,29 @@ def serving_protocols(seed: int = 1004, n_slices: int = 2) -> list[dict]:
                         oversamp=1.0, kernel_width=2, kernel_shape="circle", precision=1, lamda=1e-2,
                         max_iter=20))
     return out
+
+
+def t2_subspace_basis(n_frames: int = 500, rank: int = 4, n_atoms: int = 200, te_ms: float = 1.0,
+                      seed: int = 1005) -> np.ndarray:
+    """Rank-``rank`` temporal basis ``(rank, n_frames)`` complex64: leading right singular
+    vectors of a seeded dictionary of mono-exponential decays, T2 ~ U(20, 300) ms."""
+    rng = np.random.default_rng(seed)
+    t2 = rng.uniform(20.0, 300.0, n_atoms)
+    t = (np.arange(n_frames) + 1) * te_ms
+    D = np.exp(-t[None, :] / t2[:, None])
+    _, _, vh = np.linalg.svd(D, full_matrices=False)
+    return vh[:rank].astype(np.complex64)
+
+
+def subspace_protocol(seed: int = 1006, n_frames: int = 500, readout: int = 256, n: int = 192,
+                      coils: int = 8, rank: int = 4) -> dict:
+    """Served subspace protocol: one golden-angle spoke per frame, ``n_frames`` frames,
+    rank-``rank`` T2 basis on the frame axis (keyword set for ``ReconProtocol``)."""
+    rng = np.random.default_rng(seed)
+    coords = radial2d(n_frames, readout, n / 2.0).reshape(n_frames, readout, 2)
+    img = ellipse_phantom2d(n, rng)
+    maps = gaussian_coils((n, n), coils, rng)
+    acr = center_crop(centered_fft(maps * img, axes=(-2, -1)), 24, 2).astype(np.complex64)
+    return dict(name="sub", shape=(n, n), coords=coords, acr=acr, smaps=maps.astype(np.complex64), oversamp=2.0,
+                kernel_width=2, kernel_shape="circle", precision=1, lamda=1e-2, max_iter=20,
+                basis=t2_subspace_basis(n_frames, rank), encoding_axis=-3)

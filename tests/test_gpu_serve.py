@@ -95,3 +95,30 @@ def test_memory_budget_limits_batches(cuda):
     assert rep["requests"] == 16
     for r in reqs:  # admission never put more requests in flight than the budget holds
         assert r.batch <= (2 * one + 1) // protos[r.protocol].bytes_per_request()
+
+
+def test_subspace_requests_in_the_mix(cuda):
+    from pygrog_b200.workloads import t2_subspace_basis
+
+    rng = np.random.default_rng(21)
+    T, ro, n, C = 24, 64, 32, 4
+    coords = radial2d(T, ro, n / 2.0).reshape(T, ro, 2)
+    acr = (rng.standard_normal((C, 12, 12)) + 1j * rng.standard_normal((C, 12, 12))).astype(np.complex64)
+    maps = gaussian_coils((n, n), C, rng).astype(np.complex64)
+    sub = ReconProtocol("sub", (n, n), coords, acr, maps, oversamp=2.0, max_iter=8,
+                        basis=t2_subspace_basis(T, 3), encoding_axis=-3, device=cuda)
+    protos = {"sub": sub, **_protocols(cuda)}
+    server = ReconServer(protos, mem_budget=2 << 30, max_batch=3, n_slots=2, device=cuda)
+    reqs = _requests(protos, 12, np.random.default_rng(22))
+    rep = server.run(reqs, realtime=False)
+    assert rep["mean_batch"] > 1.0
+    for r in reqs:
+        p = protos[r.protocol]
+        alone = p.recon(r.data.to(cuda).unsqueeze(0), 0)[0].cpu()
+        assert r.result.shape == alone.shape
+        assert rel_l2(r.result.numpy(), alone.numpy()) < 1e-5
+    r = next(q for q in reqs if q.protocol == "sub")
+    sparse = sub.interp.interpolate(r.data.to(cuda).unsqueeze(0))
+    ref = sub.op.solve(sparse.reshape(sub.C, *sub.natural_shape), method="cg", max_iter=sub.max_iter,
+                       damp=sub.damp, tol=0.0)
+    assert rel_l2(r.result.numpy(), ref.cpu().numpy()) < 1e-5
