@@ -348,7 +348,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--table-mode", default=None, choices=["v6", "v5", "v3", "smem", "factored", "global"])
+    ap.add_argument("--table-mode", default=None, choices=["v8", "v8full", "v6", "v5", "v3", "smem", "factored", "global"])
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
@@ -428,8 +428,8 @@ def main():
 
     # algorithmic bytes per launch (both directions): samples + per-replica metadata + grid
     alg_bytes = N * C * 8 * B + bp.n_valid * 12 + G * C * 8 * B
-    kname = {"v6": "v6_kernel", "v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(bp.mode, "factored_kernel")
-    dom = f"grog_grid_{kname}" if fwd_ms >= adj_ms else f"grog_degrid_{kname}"
+    k_fwd, k_adj = bp.kernel_names()
+    dom = k_fwd if fwd_ms >= adj_ms else k_adj
     dom_ms = max(fwd_ms, adj_ms)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
@@ -494,7 +494,7 @@ def main():
                              else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "kernels": list(bp.kernel_names()), "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
             "fwd_ms": fwd_ms,

@@ -301,6 +301,22 @@ PGB_API int pgb_grog_degrid_v6(const void* grid, int64_t G, void* out, int64_t N
                                const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);
 
+/* One-lane-per-replica variants on the v6 plan (C <= 16; plan sub_cap <= 256:
+ * one replica per thread of a 256-thread CTA, ordered by (outer, inner, cell)
+ * inside each sub-chunk).  inner / outer (forward) and inner_h / outer_h
+ * (adjoint): row-major (n, C, C) operators (inner = whole table when
+ * n_outer == 1).  Same contract as pgb_grog_grid_v6 / pgb_grog_degrid_v6.
+ * Shared memory: pgb_grog_v8_smem_bytes(C, cells, n_inner, n_outer, sub_cap). */
+PGB_API size_t pgb_grog_v8_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer,
+                                      int64_t sub_cap);
+PGB_API int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const void* inner,
+                             int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
+                             const pgb_v6_plan* plan, void* stream);
+PGB_API int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h,
+                               int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C, int64_t B,
+                               const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
+                               const int32_t* zero_src, int64_t n_zero, void* stream);
+
 /* Replica expansion of interpolate() (calib/_grog.py:668-695):
  * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]
  * data (B,C,N), out (B,C,N*kw); entries outside [0,K) give 0. C <= 32. */

@@ -123,6 +123,8 @@ _SIGS = {
     "pgb_cg_update_xr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp],
     "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
+    "pgb_grog_grid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
+    "pgb_grog_degrid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
     "pgb_subspace_scatter": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_subspace_gather": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_psf_apply_kk": [_vp, _vp, _i64, _i64, _i64, _i64, _vp],
@@ -138,6 +140,7 @@ _SIZE_FUNCS = {
     "pgb_grog_v3_smem_bytes": [_i64, _i64, _i64, _i32],
     "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
     "pgb_grog_v6_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
+    "pgb_grog_v8_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_reduce_scratch_bytes": [],
 }
 

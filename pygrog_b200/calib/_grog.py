@@ -447,6 +447,9 @@ class GrogGridder:
     """Fused GROG gridding operator for one trajectory: brick plans + tables.
 
     Kernel families (chosen from the shared-memory budget of one CTA):
+      ``"v8"``        C <= 16: one lane per replica on balanced sub-chunk
+                      streams, replicas ordered (outer, inner, cell) so
+                      operator loads are conflict-free or broadcast;
       ``"v6"``        C <= 16: operator-stationary slots (outer factor rows
                       in registers along sorted runs, inner factor or whole
                       table in shared memory), dynamic work queue;
@@ -488,9 +491,40 @@ class GrogGridder:
             cells = br[0] * br[1] * br[2]
             return lib.pgb_grog_v6_smem_bytes(C, cells, n_in, n_out, sub) <= _SMEM_V3
 
+        def v8_fits(n_in, n_out, br, sub):
+            cells = br[0] * br[1] * br[2]
+            return lib.pgb_grog_v8_smem_bytes(C, cells, n_in, n_out, sub) <= _SMEM_V3
+
         chosen = None
         self.sub_cap = None
-        if mode in (None, "v6") and C <= 16:
+        self.fwd6 = None  # (brick, sub_cap, factored) of the v6 forward used with the v8 adjoint
+        if mode in (None, "v8", "v8full") and C <= 16:
+            n_out_f = int(factors[0].shape[0]) if factors is not None else None
+            for sub in (256, 192, 128):
+                for br in cand:
+                    if K <= 65535 and v8_fits(K, 1, br, sub):
+                        chosen = ("v8", br, False)
+                    elif n_fact is not None and n_fact <= 65535 and v8_fits(n_fact, n_out_f, br, sub):
+                        chosen = ("v8", br, True)
+                    if chosen is not None:
+                        self.sub_cap = sub
+                        break
+                if chosen is not None:
+                    break
+            if chosen is not None and mode != "v8full":
+                # the operator-stationary v6 forward is faster in dense k-space
+                # (lane-per-replica shared atomics collide on hot cells): use it
+                # when it fits with the same table factoring
+                fact8 = chosen[2]
+                for sub6 in (128, 96, 64):
+                    for br6 in cand:
+                        ok = (v6_fits(n_fact, n_out_f, br6, sub6) if fact8 else v6_fits(K, 1, br6, sub6))
+                        if ok:
+                            self.fwd6 = (br6, sub6, fact8)
+                            break
+                    if self.fwd6 is not None:
+                        break
+        if chosen is None and mode in (None, "v6") and C <= 16:
             n_out_f = int(factors[0].shape[0]) if factors is not None else None
             for sub in (128, 96, 64):
                 for br in cand:
@@ -521,7 +555,7 @@ class GrogGridder:
                     chosen = ("v3", br, True)
                     break
         if chosen is None:
-            if mode in ("v3", "v5", "v6"):
+            if mode in ("v3", "v5", "v6", "v8", "v8full"):
                 raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
             br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
                 (4, 8, 8) if ndim == 3 else (1, 16, 16))
@@ -550,7 +584,22 @@ class GrogGridder:
             self.inner = torch.as_tensor(table).to(dev).contiguous()
             self.inner_h = self.inner.conj().transpose(-1, -2).contiguous()
             self.outer = self.outer_h = None
-        self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6)
+        self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6 / v8)
+        if self.mode == "v8":
+            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap)
+            if self.fwd6 is not None:
+                br6, sub6, _ = self.fwd6
+                self.inner_lc = lane_chunk(self.inner)
+                self.outer_lc = lane_chunk(self.outer) if self.outer is not None else None
+                self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, brick=br6,
+                                       n_outer=self.n_outer, sub_cap=sub6)
+            else:
+                self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, **kw8)
+            first = _first_valid_mask(target_idx, kw)
+            self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kw8)
+            if self.plan.n_valid > self.adj_plan.n_valid:
+                self.plan2 = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kw8)
+            return
         if self.mode == "v6":
             self.inner_lc = lane_chunk(self.inner)
             self.inner_h_lc = lane_chunk(self.inner_h)
@@ -578,13 +627,21 @@ class GrogGridder:
     def n_valid(self):
         return self.plan.n_valid
 
+    def kernel_names(self) -> tuple[str, str]:
+        """Names of the (forward, adjoint) main kernels of this gridder."""
+        m = self.mode
+        if m == "v8":
+            return ("grog_grid_v6_kernel" if self.fwd6 is not None else "grog_grid_v8_kernel", "grog_degrid_v8_kernel")
+        k = {"v6": "v6_kernel", "v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(m, "factored_kernel")
+        return f"grog_grid_{k}", f"grog_degrid_{k}"
+
     def launches_per_call(self, adjoint: bool) -> int:
         bp = self.plan
         if adjoint:
-            if self.mode in ("v3", "v5", "v6"):
+            if self.mode in ("v3", "v5", "v6", "v8"):
                 return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
             return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
-        if self.mode == "v6":
+        if self.mode in ("v6", "v8"):
             return 1 + (1 if bp.zero_bricks.numel() else 0)
         return 1 + (1 if bp.split_bricks.numel() else 0)
 
@@ -598,7 +655,14 @@ class GrogGridder:
         G = out.shape[-1]
         bp = self.plan
         st = _lib.stream_ptr(data.device)
-        if self.mode == "v6":
+        if self.mode == "v8" and self.fwd6 is not None:
+            olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
+            _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
+                      self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
+        elif self.mode == "v8":
+            _lib.call("pgb_grog_grid_v8", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
+                      self.inner.shape[0], self._outer_ptr(False), self.n_outer, C, B, _ctypes_ref(bp._c), st)
+        elif self.mode == "v6":
             olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
             _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
                       self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
@@ -618,7 +682,12 @@ class GrogGridder:
         bp = self.adj_plan
         st = _lib.stream_ptr(grid.device)
         zs = bp.zero_src.data_ptr() if bp.zero_src.numel() else None
-        if self.mode == "v6":
+        if self.mode == "v8":
+            sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
+            _lib.call("pgb_grog_degrid_v8", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
+                      self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,
+                      _ctypes_ref(bp._c), sec, zs, int(bp.zero_src.numel()), st)
+        elif self.mode == "v6":
             sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
             olc = self.outer_h_lc.data_ptr() if self.outer_h_lc is not None else None
             _lib.call("pgb_grog_degrid_v6", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h_lc.data_ptr(),
