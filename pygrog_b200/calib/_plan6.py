@@ -61,6 +61,7 @@ class BrickPlan6:
         sub_cap: int = 256,
         item_subs: int = 8,
         n_cta: int | None = None,
+        lane_order: bool = False,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -124,10 +125,25 @@ class BrickPlan6:
         ubeg = torch.cumsum(ucnt, 0) - ucnt
         slot = inv - ubeg[sub_id]
 
-        # (2) order inside a sub-chunk: (outer, inner, cell)
+        # (2) order inside a sub-chunk: (outer, inner, cell); with lane_order
+        # (one replica per lane), inside each outer run the replicas are dealt
+        # round-robin over the eight residues q mod 8, so eight consecutive lanes
+        # read eight inner operators that start in different bank quads
         n_in = int(q.max()) + 1 if n else 1
         key2 = ((sub_id * self.n_outer + k) * n_in + q) * cells + cl
         _, p2 = torch.sort(key2, stable=True)
+        if lane_order and n:
+            res = q[p2] % 8
+            grp = (sub_id[p2] * self.n_outer + k[p2]) * 8 + res
+            _, pg = torch.sort(grp, stable=True)  # inside a group still (q, cell) order
+            gs = grp[pg]
+            gcnt = torch.bincount(gs)
+            gstart = torch.cumsum(gcnt, 0) - gcnt
+            rank = torch.arange(n, device=dev) - gstart[gs]
+            sk = sub_id[p2][pg] * self.n_outer + k[p2][pg]
+            key3 = (sk * (self.sub_cap + 1) + rank) * 8 + res[pg]
+            _, p3 = torch.sort(key3, stable=True)
+            p2 = p2[pg][p3]
         sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
         self.meta = torch.stack([cl | (slot << 16), q | (k << 16)], dim=1).to(torch.int32).contiguous()
         self.w = w.contiguous()

@@ -85,6 +85,7 @@ class ReconProtocol:
         self.max_iter = int(max_iter)
         self.damp = float(damp)
         self._solvers: dict = {}
+        self._io: dict = {}  # slot -> (device input, page-locked output), allocated once
         self._cap = 1
 
     @property
@@ -107,6 +108,8 @@ class ReconProtocol:
         for s in range(n_slots):
             self._solvers[s] = BatchedDeviceCG(self.op, self._cap, self.image_shape, self.device,
                                                damp=self.damp, tol=0.0)
+            self._io[s] = (torch.empty((self._cap, *self.data_shape), dtype=torch.complex64, device=self.device),
+                           torch.empty((self._cap, *self.image_shape), dtype=torch.complex64, pin_memory=True))
         x = torch.zeros(max_batch, *self.data_shape, dtype=torch.complex64, device=self.device)
         for F in range(1, max_batch + 1):
             self.recon(x[:F], 0, max_iter=1)
@@ -160,11 +163,12 @@ class ReconServer:
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
             F = len(reqs)
-            d = torch.empty((F, *proto.data_shape), dtype=torch.complex64, device=self.device)
+            d_all, h_all = proto._io[slot]  # the slot's buffers: free while the slot is free
+            d = d_all[:F]
             for i, r in enumerate(reqs):
                 d[i].copy_(r.data, non_blocking=True)
             x = proto.recon(d, slot)
-            host = torch.empty(tuple(x.shape), dtype=torch.complex64, pin_memory=True)
+            host = h_all[:F]
             host.copy_(x, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(s)

@@ -210,3 +210,35 @@ def test_brick_plan6_invariants(shape, brick, n_outer, sub_cap):
     assert lc[3, 7, 4, 1] == M[3, 4 * 2 + 1, 7]
     lc5 = lane_chunk(torch.randn(2, 5, 5, dtype=torch.complex64))
     assert lc5.shape == (2, 5, 5, 1)
+
+
+def test_brick_plan6_lane_order_deals_residues():
+    from pygrog_b200.calib._plan6 import BrickPlan6
+
+    rng = np.random.default_rng(9)
+    shape, kw = (24, 16, 40), 3
+    tgt, _, w = _toy_plan(shape, 6000, kw, rng, hot=3000)
+    idx = torch.from_numpy(rng.integers(0, 11 * 121, size=(6000, kw)).astype(np.int64))
+    a = BrickPlan6(tgt, idx, w, kw, shape, (4, 8, 8), n_outer=11, sub_cap=256, n_cta=3)
+    b = BrickPlan6(tgt, idx, w, kw, shape, (4, 8, 8), n_outer=11, sub_cap=256, n_cta=3, lane_order=True)
+    assert torch.equal(a.subs, b.subs) and torch.equal(a.uniq, b.uniq)
+    def conflict_degree(m):
+        """Mean over aligned groups of eight lanes of the largest number of
+        distinct inner operators sharing one residue q mod 8."""
+        q = m[:, 1] & 0xFFFF
+        out = []
+        for g0 in range(0, len(q) - 7, 8):
+            qs = set(q[g0:g0 + 8].tolist())
+            out.append(max(np.bincount([v % 8 for v in qs], minlength=8)))
+        return np.mean(out)
+
+    da, db = [], []
+    for r0, r1, _, _ in b.subs.numpy():
+        ma = a.meta.numpy()[r0:r1].astype(np.int64)
+        mb = b.meta.numpy()[r0:r1].astype(np.int64)
+        assert sorted(map(tuple, ma.tolist())) == sorted(map(tuple, mb.tolist()))  # same replicas
+        assert np.all(np.diff(mb[:, 1] >> 16) >= 0)  # outer runs kept together
+        if r1 - r0 >= 64:
+            da.append(conflict_degree(ma))
+            db.append(conflict_degree(mb))
+    assert np.mean(db) < np.mean(da)
