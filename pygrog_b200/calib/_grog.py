@@ -464,6 +464,9 @@ class GrogGridder:
     """
 
     BRICKS3 = ((8, 8, 8), (4, 8, 8), (4, 4, 8), (2, 4, 8))
+    # v8 plans: deal replicas round-robin over inner residues q mod 8 inside
+    # outer runs (BrickPlan6 lane_order): fewer shared-memory bank conflicts
+    LANE_ORDER_V8 = True
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
 
     def __init__(self, target_idx, interp_idx, rep_weight, kw, grid_shape, table, factors, nsteps,
@@ -586,7 +589,7 @@ class GrogGridder:
             self.outer = self.outer_h = None
         self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6 / v8)
         if self.mode == "v8":
-            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap)
+            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap, lane_order=self.LANE_ORDER_V8)
             if self.fwd6 is not None:
                 br6, sub6, _ = self.fwd6
                 self.inner_lc = lane_chunk(self.inner)
