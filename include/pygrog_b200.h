@@ -287,6 +287,12 @@ typedef struct pgb_v6_plan {
   int32_t nbz, nby, nbx;
   const int32_t* zero_bricks;
   int32_t n_zero_bricks;
+  /* cell order of every sub-chunk, for the lane-per-replica forward (may be
+   * NULL otherwise): entry = pos | cell << 9 | head << 21 | shared << 22,
+   * sorted by (cell, pos) inside the sub-chunk, pos = index of the replica in
+   * it; a head starts a segment of entries of one cell (summed by one thread),
+   * shared marks segments of a cell that has several (added atomically) */
+  const int32_t* cword;
 } pgb_v6_plan;
 
 PGB_API size_t pgb_grog_v6_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer,

@@ -48,6 +48,7 @@ class V6PlanC(ctypes.Structure):
         ("nbx", ctypes.c_int32),
         ("zero_bricks", _vp),
         ("n_zero_bricks", ctypes.c_int32),
+        ("cword", _vp),
     ]
 
 

@@ -449,7 +449,9 @@ class GrogGridder:
     Kernel families (chosen from the shared-memory budget of one CTA):
       ``"v8"``        C <= 16: one lane per replica on balanced sub-chunk
                       streams, replicas ordered (outer, inner, cell) so
-                      operator loads are conflict-free or broadcast;
+                      operator loads are conflict-free or broadcast; the
+                      forward sums each cell's replicas without atomics;
+      ``"v8pair"``    the v8 adjoint with the v6 forward;
       ``"v6"``        C <= 16: operator-stationary slots (outer factor rows
                       in registers along sorted runs, inner factor or whole
                       table in shared memory), dynamic work queue;
@@ -467,6 +469,8 @@ class GrogGridder:
     # v8 plans: deal replicas round-robin over inner residues q mod 8 inside
     # outer runs (BrickPlan6 lane_order): fewer shared-memory bank conflicts
     LANE_ORDER_V8 = True
+    # v8 forward: longest run of one cell's replicas summed by one thread
+    SEG_LEN_V8 = 24
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
 
     def __init__(self, target_idx, interp_idx, rep_weight, kw, grid_shape, table, factors, nsteps,
@@ -501,7 +505,7 @@ class GrogGridder:
         chosen = None
         self.sub_cap = None
         self.fwd6 = None  # (brick, sub_cap, factored) of the v6 forward used with the v8 adjoint
-        if mode in (None, "v8", "v8full") and C <= 16:
+        if mode in (None, "v8", "v8pair") and C <= 16:
             n_out_f = int(factors[0].shape[0]) if factors is not None else None
             for sub in (256, 192, 128):
                 for br in cand:
@@ -514,10 +518,8 @@ class GrogGridder:
                         break
                 if chosen is not None:
                     break
-            if chosen is not None and mode != "v8full":
-                # the operator-stationary v6 forward is faster in dense k-space
-                # (lane-per-replica shared atomics collide on hot cells): use it
-                # when it fits with the same table factoring
+            if chosen is not None and mode == "v8pair":
+                # the operator-stationary v6 forward with the same table factoring
                 fact8 = chosen[2]
                 for sub6 in (128, 96, 64):
                     for br6 in cand:
@@ -558,7 +560,7 @@ class GrogGridder:
                     chosen = ("v3", br, True)
                     break
         if chosen is None:
-            if mode in ("v3", "v5", "v6", "v8", "v8full"):
+            if mode in ("v3", "v5", "v6", "v8", "v8pair"):
                 raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
             br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
                 (4, 8, 8) if ndim == 3 else (1, 16, 16))
@@ -597,7 +599,8 @@ class GrogGridder:
                 self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, brick=br6,
                                        n_outer=self.n_outer, sub_cap=sub6)
             else:
-                self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, **kw8)
+                self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_order=True,
+                                       seg_len=self.SEG_LEN_V8, **kw8)
             first = _first_valid_mask(target_idx, kw)
             self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kw8)
             if self.plan.n_valid > self.adj_plan.n_valid:

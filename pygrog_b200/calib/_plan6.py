@@ -43,6 +43,10 @@ class BrickPlan6:
       ``sd`` / ``si`` / ``cta_ptr``  per-CTA sub-chunk streams: descriptor,
                  ``{brick, flags}`` (1 first of item, 2 last, 4 split brick)
       ``work``   (host) int32 (n_items, 5) ``{brick, sub_begin, sub_end, split, cta}``
+      ``cword``  int32, with ``cell_order``: each sub-chunk's replicas in cell
+                 order, ``pos | cell << 9 | head << 21 | shared << 22``; a
+                 head starts a segment of at most ``seg_len`` replicas of one
+                 cell, ``shared`` marks segments of a cell with several
       ``zero_bricks`` bricks the forward zeroes first (empty and split)
       ``zero_src`` samples with no replica in this plan; ``multi`` whether a
       sample has more than one.
@@ -62,6 +66,8 @@ class BrickPlan6:
         item_subs: int = 8,
         n_cta: int | None = None,
         lane_order: bool = False,
+        cell_order: bool = False,
+        seg_len: int = 8,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -154,6 +160,34 @@ class BrickPlan6:
         self.n_valid = n
         self.n_subs = n_subs
         self.rep_src = src.to(torch.int32)  # replica -> sample, in kernel order (host checks)
+        # cell order of each sub-chunk (lane-per-replica forward): entries
+        # sorted by (cell, pos), pos = the replica's index inside the sub-chunk;
+        # a cell's run is cut into near-equal segments of at most seg_len entries, each
+        # summed by one thread (bounded serial work in dense k-space), and
+        # segments of a cell with several are added to the tile atomically
+        self.cword = torch.zeros(0, dtype=torch.int32, device=dev)
+        if cell_order and n:
+            if self.sub_cap > 512 or cells > 4096:
+                raise ValueError("cell order needs sub_cap <= 512 and cells <= 4096")
+            if seg_len < 1:
+                raise ValueError("seg_len must be >= 1")
+            pos_in = torch.arange(n, device=dev) - rbeg[sub_id]
+            _, pc = torch.sort(sub_id * (cells * 512) + cl * 512 + pos_in, stable=True)
+            c_s, s_s = cl[pc], sub_id[pc]
+            first_c = torch.ones(n, dtype=torch.bool, device=dev)
+            first_c[1:] = (c_s[1:] != c_s[:-1]) | (s_s[1:] != s_s[:-1])
+            run_id = torch.cumsum(first_c.to(torch.int64), 0) - 1
+            run_len = torch.bincount(run_id)
+            run_beg = torch.cumsum(run_len, 0) - run_len
+            in_run = torch.arange(n, device=dev) - run_beg[run_id]
+            # a run of L entries -> ceil(L / seg_len) near-equal segments
+            L = run_len[run_id]
+            parts = (L + seg_len - 1) // seg_len
+            part = in_run * parts // L
+            head = (in_run == 0) | (part != (in_run - 1).clamp(min=0) * parts // L)
+            shared = parts > 1
+            self.cword = (pos_in[pc] | (c_s << 9) | (head.to(torch.int64) << 21)
+                          | (shared.to(torch.int64) << 22)).to(torch.int32).contiguous()
 
         # (3) brick items of at most item_subs sub-chunks, assigned largest
         # first to the least loaded CTA; each CTA gets a flat sub-chunk stream
@@ -184,7 +218,8 @@ class BrickPlan6:
         per_cta = np.bincount(cta[ent_item], minlength=n_cta) if ent_item.size else np.zeros(n_cta, np.int64)
         self.cta_ptr = torch.from_numpy(np.concatenate([[0], np.cumsum(per_cta)]).astype(np.int32)).to(dev)
         self.n_cta = n_cta
-        self.cta_cost = np.bincount(cta, weights=reps + cells // 4, minlength=n_cta) if len(cta) else np.zeros(n_cta)
+        self.cta_cost = (np.bincount(cta, weights=(reps + cells // 4)[order], minlength=n_cta) if len(cta)
+                         else np.zeros(n_cta))
         split_b = nit_b > 1
         self.split_bricks = torch.nonzero(split_b).squeeze(1).to(torch.int32).contiguous()
         self.zero_bricks = torch.nonzero(split_b | (cnt == 0)).squeeze(1).to(torch.int32).contiguous()
@@ -204,7 +239,7 @@ class BrickPlan6:
         return _lib.V6PlanC(
             ptr(self.sd), ptr(self.si), self.cta_ptr.data_ptr(), self.n_cta if self.sd.numel() else 0,
             ptr(self.uniq), ptr(self.meta), ptr(self.w), self.sub_cap, gz, gy, gx, bz, by, bx, nbz, nby, nbx,
-            ptr(self.zero_bricks), int(self.zero_bricks.numel()),
+            ptr(self.zero_bricks), int(self.zero_bricks.numel()), ptr(self.cword),
         )
 
 

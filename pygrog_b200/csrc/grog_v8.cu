@@ -11,7 +11,9 @@
 // lane keeps its replica's source coils, intermediate and result in
 // registers; the tables live in shared memory, row-major per operator.
 //
-//   forward:  y = O[k] (I[q] x_src)          tile[:, cell] += w y (shared atomics)
+//   forward:  y = O[k] (I[q] x_src); w y goes to the staging buffer, then one
+//             owner thread per cell sums the cell's replicas (plan cell order)
+//             and updates tile[:, cell] with plain loads and stores
 //   adjoint:  y = I^H[q] (O^H[k] tile[cell]) result[:, slot] = w y
 //
 // Streams as in grog_v6.cu: every CTA walks its own list of sub-chunk
@@ -61,17 +63,19 @@ __device__ __forceinline__ bool flat8(const Geom8& g, int z0, int y0, int x0, in
 __host__ __device__ constexpr int even8(int v) { return (v + 1) & ~1; }
 
 // Shared memory in float2 units:
-//   inner table | outer table | tiles[T] | staging / results (X buffers of C x sub_cap, coil-major)
+//   inner table | outer table | tiles[T] | staging / results (X buffers of C x sub_cap, coil-major) |
+//   forward: cell-order words of the current sub-chunk (sub_cap int32)
 template <int C>
 struct Smem8 {
-  int tin, tout, tile, tile_sz, xs, total;
+  int tin, tout, tile, tile_sz, xs, cw, total;
   __host__ __device__ Smem8(int n_inner, int n_outer, int cells, int sub_cap, bool forward) {
     tin = 0;
     tout = n_inner * Pad8<C>::OPS;
     tile = tout + (n_outer > 1 ? n_outer * Pad8<C>::OPS : 0);
     tile_sz = even8(forward ? C * (cells + 1) : cells * C);
     xs = tile + (forward ? 1 : 2) * tile_sz;
-    total = xs + (forward ? 2 : 1) * C * sub_cap;
+    cw = xs + (forward ? 2 : 1) * C * sub_cap;
+    total = cw + (forward ? (sub_cap + 1) / 2 : 0);  // forward: cell-order words of the sub-chunk
   }
 };
 
@@ -191,8 +195,8 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
     const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G,
     const float2* __restrict__ inner, int n_inner, const float2* __restrict__ outer, int n_outer,
     const int4* __restrict__ sd, const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr,
-    const int32_t* __restrict__ uniq, const int2* __restrict__ meta, const float* __restrict__ wts, int cap,
-    Geom8 geom) {
+    const int32_t* __restrict__ uniq, const int2* __restrict__ meta, const float* __restrict__ wts,
+    const int32_t* __restrict__ cword, int cap, Geom8 geom) {
   extern __shared__ float4 smem4[];
   constexpr int OPS = Pad8<C>::OPS;
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
@@ -203,11 +207,11 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
   float2* base = reinterpret_cast<float2*>(smem4);
   float2* tin = base + lay.tin;
   float2* tout = base + lay.tout;
-  // tile as separate real / imaginary planes (C, TS) each, TS odd: the 32
-  // lanes' atomics on one coil spread over all banks
+  // tile as separate real / imaginary planes (C, TS) each
   float* tre = reinterpret_cast<float*>(base + lay.tile);
   float* tim = tre + C * TS;
-  float2* xs0 = base + lay.xs;     // 2 x (C, cap)
+  float2* xs0 = base + lay.xs;  // 2 x (C, cap): staged sample coils, then this sub-chunk's results
+  int32_t* cws = reinterpret_cast<int32_t*>(base + lay.cw);
   const int b = blockIdx.y;
   const float2* dat = data + static_cast<int64_t>(b) * C * N;
   float2* grd = grid + static_cast<int64_t>(b) * C * G;
@@ -225,6 +229,10 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
   float w0, w1;
   ld_rep8(meta, wts, st.d0, cap, m0, w0);
   ld_rep8(meta, wts, st.d1, cap, m1, w1);
+  auto ld_cw = [&](int4 d, bool valid) -> int32_t {
+    return (valid && tid < nrp8(d, cap)) ? __ldg(cword + d.x + tid) : 0;
+  };
+  int32_t c0 = ld_cw(st.d0, true), c1 = ld_cw(st.d1, st.p + 1 < p1);
   stage_ops8<C>(tin, inner, n_inner);
   if (OUTER) stage_ops8<C>(tout, outer, n_outer);
   for (int t = tid; t < 2 * C * TS; t += kT8) tre[t] = 0.f;
@@ -244,17 +252,19 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
     int2 m2;
     float w2;
     ld_rep8(meta, wts, st.p + 2 < p1 ? st.d2 : make_int4(0, 0, 0, 0), cap, m2, w2);
+    const int32_t c2 = ld_cw(st.d2, st.p + 2 < p1);
     __syncthreads();  // staging buffer `buf` complete; tile zeroed
     {
+      const int nr = nrp8(st.d0, cap);
       const int nu = nsl8(st.d0, cap);
       const int cell = m0.x & 0xFFFF;
       const int sl = static_cast<int>(static_cast<unsigned>(m0.x) >> 16);
       const int q = m0.y & 0xFFFF;
       const int k = static_cast<int>(static_cast<unsigned>(m0.y) >> 16);
       const bool on = m0.x >= 0 && cell < cells && sl < nu && q < n_inner && (OUTER ? k < n_outer : k == 0);
+      float2* xs = xs0 + buf * C * cap;
+      float2 x[C], u[C];
       if (on) {
-        const float2* xs = xs0 + buf * C * cap;
-        float2 x[C], u[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) x[c] = xs[c * cap + sl];
         matvec8<C>(tin + q * OPS, x, u);
@@ -263,14 +273,58 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
 #pragma unroll
           for (int c = 0; c < C; ++c) u[c] = x[c];
         }
+      }
+      __syncthreads();  // every lane has read its staged coils: the buffer takes the results
+      if (tid < nr) {
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-          atomicAdd(tre + c * TS + cell, w0 * u[c].x);
-          atomicAdd(tim + c * TS + cell, w0 * u[c].y);
+        for (int c = 0; c < C; ++c)
+          xs[c * cap + tid] = on ? make_float2(w0 * u[c].x, w0 * u[c].y) : make_float2(0.f, 0.f);
+        cws[tid] = c0;
+      }
+      __syncthreads();
+      // one owner per segment (the head of at most a few entries of one cell
+      // in cell order) sums the segment's results and updates the tile; only
+      // segments of a cell with several add atomically
+      if (tid < nr && ((c0 >> 21) & 1)) {
+        const int cl = (c0 >> 9) & 4095;
+        float2 acc[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = make_float2(0.f, 0.f);
+        int j = tid, wj = c0;
+        while (true) {
+          const int pos = wj & 511;
+          if (pos < nr) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              const float2 v = xs[c * cap + pos];
+              acc[c].x += v.x;
+              acc[c].y += v.y;
+            }
+          }
+          if (++j >= nr) break;
+          wj = cws[j];
+          if ((wj >> 21) & 1) break;
+        }
+        if (cl < cells) {
+          if ((c0 >> 22) & 1) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              atomicAdd(tre + c * TS + cl, acc[c].x);
+              atomicAdd(tim + c * TS + cl, acc[c].y);
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              tre[c * TS + cl] += acc[c].x;
+              tim[c * TS + cl] += acc[c].y;
+            }
+          }
         }
       }
     }
-    __syncthreads();  // compute done: staging buffer `buf` and the tile are free
+    // every owner is done with the results (their buffer is refilled by the
+    // next iteration's staging) and with the tile (flushed below)
+    __syncthreads();
     if (st.i0.y & kLast8) {
       int z0, y0, x0;
       origin8(geom, st.i0.x, z0, y0, x0);
@@ -301,6 +355,8 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
     w0 = w1;
     m1 = m2;
     w1 = w2;
+    c0 = c1;
+    c1 = c2;
     buf ^= 1;
   }
 }
@@ -555,6 +611,7 @@ int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const v
     PGB_LAUNCH_CHECK("grog_grid_v8(zero bricks)");
   }
   if (plan->n_cta == 0) return PGB_OK;
+  PGB_REQUIRE(plan->cword != nullptr, PGB_ERR_INVALID, "grog_grid_v8: the plan has no cell order (cword)");
   const bool has_outer = n_outer > 1;
   dim3 grd(plan->n_cta, static_cast<unsigned>(B));
   switch (C) {
@@ -567,7 +624,7 @@ int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const v
                              static_cast<const float2*>(outer), static_cast<int>(n_outer),                  \
                              reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si), \
                              plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,  \
-                             plan->sub_cap, geom);                                                          \
+                             plan->cword, plan->sub_cap, geom);                                             \
   } break;
     PGB8_FOR_EACH_C(X)
 #undef X

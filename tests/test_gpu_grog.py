@@ -96,7 +96,7 @@ def _random_case(ndim, n, spokes, readout, C, osf, kwd, ks, prec, seed, B=1):
     return coords, calib, data
 
 
-@pytest.mark.parametrize("mode", ["auto", "v8", "v8full", "v6", "v5", "v3", "global", "factored"])
+@pytest.mark.parametrize("mode", ["auto", "v8", "v8pair", "v6", "v5", "v3", "global", "factored"])
 @pytest.mark.parametrize("ndim,n,spokes,readout,C,osf,kwd,ks,prec,B", [
     (2, 64, 40, 128, 8, 1.0, 5, "square", 2, 1),   # c0-like (hot DC cell, 1 valid replica)
     (2, 48, 30, 96, 16, 2.0, 2, "circle", 1, 2),   # c2-like, several valid replicas, batch 2
@@ -111,7 +111,7 @@ def test_fused_grid_degrid_vs_oracle_radial(cuda, ndim, n, spokes, readout, C, o
     g.calc_interp_table(calib, lamda=0.01, precision=prec)
     if mode != "auto":
         g.gridder_mode = mode
-        if mode in ("v3", "v5", "v6", "v8", "v8full") and C > 16:
+        if mode in ("v3", "v5", "v6", "v8", "v8pair") and C > 16:
             pytest.skip("v3 / v5 / v6 / v8 kernels cover C <= 16")
         if mode == "factored":
             from pygrog_b200 import _lib

@@ -242,3 +242,37 @@ def test_brick_plan6_lane_order_deals_residues():
             da.append(conflict_degree(ma))
             db.append(conflict_degree(mb))
     assert np.mean(db) < np.mean(da)
+
+
+def test_brick_plan6_cell_order_words():
+    from pygrog_b200.calib._plan6 import BrickPlan6
+
+    rng = np.random.default_rng(12)
+    shape, kw = (24, 16, 40), 3
+    tgt, _, w = _toy_plan(shape, 5000, kw, rng, hot=2500)
+    idx = torch.from_numpy(rng.integers(0, 11 * 121, size=(5000, kw)).astype(np.int64))
+    seg = 4
+    bp = BrickPlan6(tgt, idx, w, kw, shape, (4, 8, 8), n_outer=11, sub_cap=256, n_cta=3, lane_order=True,
+                    cell_order=True, seg_len=seg)
+    cw = bp.cword.numpy().astype(np.int64)
+    meta = bp.meta.numpy().astype(np.int64)
+    n_shared = 0
+    for r0, r1, _, _ in bp.subs.numpy():
+        e = cw[r0:r1]
+        pos, cell, head, shared = e & 511, (e >> 9) & 4095, (e >> 21) & 1, (e >> 22) & 1
+        assert sorted(pos.tolist()) == list(range(r1 - r0))  # every replica once
+        assert np.array_equal(cell, meta[r0 + pos, 0] & 0xFFFF)  # the replica's cell
+        key = cell * 512 + pos
+        assert np.all(np.diff(key) > 0)  # sorted by (cell, pos)
+        # segments: every cell's run cut into ceil(L / seg) parts of near-equal size
+        new_cell = np.concatenate([[1], (np.diff(cell) != 0).astype(int)])
+        starts = np.flatnonzero(new_cell)
+        run_len = np.diff(np.append(starts, len(cell)))
+        for s0, L in zip(starts, run_len):
+            h = np.flatnonzero(head[s0:s0 + L])
+            sizes = np.diff(np.append(h, L))
+            assert h[0] == 0 and sizes.max() <= seg and sizes.max() - sizes.min() <= 1
+            assert len(h) == -(-L // seg)
+            assert np.all(shared[s0:s0 + L] == (L > seg))
+        n_shared += int(shared.sum())
+    assert n_shared > 0  # the hot cells give runs longer than a segment
