@@ -47,6 +47,9 @@ class BrickPlan6:
                  order, ``pos | cell << 9 | head << 21 | shared << 22``; a
                  head starts a segment of at most ``seg_len`` replicas of one
                  cell, ``shared`` marks segments of a cell with several
+      ``n_pad``  padding entries (``lane_order`` only: meta ``-1``, weight 0,
+                 cell order cell = ``cells``) that round every sub-chunk to
+                 whole quarter-warps
       ``zero_bricks`` bricks the forward zeroes first (empty and split)
       ``zero_src`` samples with no replica in this plan; ``multi`` whether a
       sample has more than one.
@@ -131,35 +134,73 @@ class BrickPlan6:
         ubeg = torch.cumsum(ucnt, 0) - ucnt
         slot = inv - ubeg[sub_id]
 
-        # (2) order inside a sub-chunk: (outer, inner, cell); with lane_order
-        # (one replica per lane), inside each outer run the replicas are dealt
-        # round-robin over the eight residues q mod 8, so eight consecutive lanes
-        # read eight inner operators that start in different bank quads
+        # (2) order inside a sub-chunk: (outer, inner, cell).  With lane_order
+        # (one replica per lane) the sub-chunk is laid out in residue columns:
+        # replicas bucketed by r = q mod 8 (inner operator q starts in bank quad
+        # r), the i-th of bucket r on lane 8 i + r, so the eight lanes of a
+        # quarter-warp read inner operators in eight different bank quads;
+        # buckets ordered by (outer, inner, cell) keep the outer indices of a
+        # quarter-warp equal or adjacent.  ceil(n / 8) quarter-warps per
+        # sub-chunk: the overflow of long buckets fills the holes of short ones,
+        # remaining holes are padding entries (meta -1, weight 0).
         n_in = int(q.max()) + 1 if n else 1
-        key2 = ((sub_id * self.n_outer + k) * n_in + q) * cells + cl
-        _, p2 = torch.sort(key2, stable=True)
+        pad = torch.zeros(0, dtype=torch.bool, device=dev)
         if lane_order and n:
-            res = q[p2] % 8
-            grp = (sub_id[p2] * self.n_outer + k[p2]) * 8 + res
-            _, pg = torch.sort(grp, stable=True)  # inside a group still (q, cell) order
-            gs = grp[pg]
-            gcnt = torch.bincount(gs)
-            gstart = torch.cumsum(gcnt, 0) - gcnt
-            rank = torch.arange(n, device=dev) - gstart[gs]
-            sk = sub_id[p2][pg] * self.n_outer + k[p2][pg]
-            key3 = (sk * (self.sub_cap + 1) + rank) * 8 + res[pg]
-            _, p3 = torch.sort(key3, stable=True)
-            p2 = p2[pg][p3]
-        sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
-        self.meta = torch.stack([cl | (slot << 16), q | (k << 16)], dim=1).to(torch.int32).contiguous()
-        self.w = w.contiguous()
+            rho = q % 8
+            key2 = ((((sub_id * 8 + rho) * self.n_outer + k) * n_in + q) * cells) + cl
+            _, p2 = torch.sort(key2, stable=True)
+            sub_id, cl, slot, q, k, w, src, rho = (a[p2] for a in (sub_id, cl, slot, q, k, w, src, rho))
+            nq = (torch.bincount(sub_id, minlength=n_subs) + 7) // 8
+            grp = sub_id * 8 + rho
+            gcnt = torch.bincount(grp, minlength=n_subs * 8)
+            rank = torch.arange(n, device=dev) - (torch.cumsum(gcnt, 0) - gcnt)[grp]
+            lane = rank * 8 + rho
+            over = rank >= nq[sub_id]
+            nslot = nq * 8
+            sbase = torch.cumsum(nslot, 0) - nslot
+            total = int(nslot.sum())
+            used = torch.zeros(total, dtype=torch.bool, device=dev)
+            used[sbase[sub_id[~over]] + lane[~over]] = True
+            holes = torch.nonzero(~used).squeeze(1)
+            hole_sub = torch.searchsorted(sbase, holes, right=True) - 1
+            hcnt = torch.bincount(hole_sub, minlength=n_subs)
+            hbeg = torch.cumsum(hcnt, 0) - hcnt
+            ov = torch.nonzero(over).squeeze(1)
+            ov_sub = sub_id[ov]
+            ocnt = torch.bincount(ov_sub, minlength=n_subs)
+            orank = torch.arange(ov.numel(), device=dev) - (torch.cumsum(ocnt, 0) - ocnt)[ov_sub]
+            dest = sbase[sub_id] + lane
+            dest[ov] = holes[hbeg[ov_sub] + orank]
+            pad = torch.ones(total, dtype=torch.bool, device=dev)
+            pad[dest] = False
+
+            def spread(v, fill):
+                out = torch.full((total,), fill, dtype=v.dtype, device=dev)
+                out[dest] = v
+                return out
+
+            sub_full = torch.searchsorted(sbase, torch.arange(total, device=dev), right=True) - 1
+            meta0 = spread(cl | (slot << 16), -1)
+            meta1 = spread(q | (k << 16), 0)
+            self.meta = torch.stack([meta0, meta1], dim=1).to(torch.int32).contiguous()
+            self.w = spread(w, 0.0).contiguous()
+            src = spread(src, -1)
+            cl = spread(cl, cells)  # padding: no cell
+            sub_id = sub_full
+        else:
+            key2 = ((sub_id * self.n_outer + k) * n_in + q) * cells + cl
+            _, p2 = torch.sort(key2, stable=True)
+            sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
+            self.meta = torch.stack([cl | (slot << 16), q | (k << 16)], dim=1).to(torch.int32).contiguous()
+            self.w = w.contiguous()
         self.uniq = (uk - uniq_sub * n_src).to(torch.int32).contiguous()
         rcnt = torch.bincount(sub_id, minlength=n_subs)
         rbeg = torch.cumsum(rcnt, 0) - rcnt
         self.subs = torch.stack([rbeg, rbeg + rcnt, ubeg, ubeg + ucnt], dim=1).to(torch.int32).contiguous()
+        self.n_pad = int(pad.sum())
         self.n_valid = n
         self.n_subs = n_subs
-        self.rep_src = src.to(torch.int32)  # replica -> sample, in kernel order (host checks)
+        self.rep_src = src.to(torch.int32)  # replica -> sample in kernel order, -1 for padding
         # cell order of each sub-chunk (lane-per-replica forward): entries
         # sorted by (cell, pos), pos = the replica's index inside the sub-chunk;
         # a cell's run is cut into near-equal segments of at most seg_len entries, each
@@ -167,25 +208,29 @@ class BrickPlan6:
         # segments of a cell with several are added to the tile atomically
         self.cword = torch.zeros(0, dtype=torch.int32, device=dev)
         if cell_order and n:
-            if self.sub_cap > 512 or cells > 4096:
-                raise ValueError("cell order needs sub_cap <= 512 and cells <= 4096")
+            if self.sub_cap > 512 or cells > 4095:
+                raise ValueError("cell order needs sub_cap <= 512 and cells <= 4095")
             if seg_len < 1:
                 raise ValueError("seg_len must be >= 1")
-            pos_in = torch.arange(n, device=dev) - rbeg[sub_id]
-            _, pc = torch.sort(sub_id * (cells * 512) + cl * 512 + pos_in, stable=True)
+            n_ent = sub_id.numel()  # replicas + padding
+            pos_in = torch.arange(n_ent, device=dev) - rbeg[sub_id]
+            _, pc = torch.sort(sub_id * ((cells + 1) * 512) + cl * 512 + pos_in, stable=True)
             c_s, s_s = cl[pc], sub_id[pc]
-            first_c = torch.ones(n, dtype=torch.bool, device=dev)
+            first_c = torch.ones(n_ent, dtype=torch.bool, device=dev)
             first_c[1:] = (c_s[1:] != c_s[:-1]) | (s_s[1:] != s_s[:-1])
             run_id = torch.cumsum(first_c.to(torch.int64), 0) - 1
             run_len = torch.bincount(run_id)
             run_beg = torch.cumsum(run_len, 0) - run_len
-            in_run = torch.arange(n, device=dev) - run_beg[run_id]
+            in_run = torch.arange(n_ent, device=dev) - run_beg[run_id]
             # a run of L entries -> ceil(L / seg_len) near-equal segments
             L = run_len[run_id]
             parts = (L + seg_len - 1) // seg_len
             part = in_run * parts // L
             head = (in_run == 0) | (part != (in_run - 1).clamp(min=0) * parts // L)
             shared = parts > 1
+            is_pad = c_s >= cells  # padding entries: one-entry segments, no tile update
+            head = head | is_pad
+            shared = shared & ~is_pad
             self.cword = (pos_in[pc] | (c_s << 9) | (head.to(torch.int64) << 21)
                           | (shared.to(torch.int64) << 22)).to(torch.int32).contiguous()
 
@@ -223,7 +268,7 @@ class BrickPlan6:
         split_b = nit_b > 1
         self.split_bricks = torch.nonzero(split_b).squeeze(1).to(torch.int32).contiguous()
         self.zero_bricks = torch.nonzero(split_b | (cnt == 0)).squeeze(1).to(torch.int32).contiguous()
-        per_src = torch.bincount(src, minlength=n_src)
+        per_src = torch.bincount(src[src >= 0], minlength=n_src)
         self.multi = bool(int(per_src.max()) > 1) if per_src.numel() else False
         self.zero_src = torch.nonzero(per_src == 0).squeeze(1).to(torch.int32).contiguous()
         self._c = self._struct()
