@@ -135,42 +135,28 @@ class BrickPlan6:
         slot = inv - ubeg[sub_id]
 
         # (2) order inside a sub-chunk: (outer, inner, cell).  With lane_order
-        # (one replica per lane) the sub-chunk is laid out in residue columns:
-        # replicas bucketed by r = q mod 8 (inner operator q starts in bank quad
-        # r), the i-th of bucket r on lane 8 i + r, so the eight lanes of a
-        # quarter-warp read inner operators in eight different bank quads;
-        # buckets ordered by (outer, inner, cell) keep the outer indices of a
-        # quarter-warp equal or adjacent.  ceil(n / 8) quarter-warps per
-        # sub-chunk: the overflow of long buckets fills the holes of short ones,
-        # remaining holes are padding entries (meta -1, weight 0).
+        # (one replica per lane) the sub-chunk is laid out in whole
+        # quarter-warps whose eight lanes read inner operators in different bank
+        # quads (inner operator q starts in quad q mod 8) or the same operator,
+        # and likewise outer ones (_pack_quarter_warps); the lanes left free are
+        # padding entries (meta -1, weight 0), fewer than eight per sub-chunk.
         n_in = int(q.max()) + 1 if n else 1
         pad = torch.zeros(0, dtype=torch.bool, device=dev)
         if lane_order and n:
-            rho = q % 8
-            key2 = ((((sub_id * 8 + rho) * self.n_outer + k) * n_in + q) * cells) + cl
-            _, p2 = torch.sort(key2, stable=True)
-            sub_id, cl, slot, q, k, w, src, rho = (a[p2] for a in (sub_id, cl, slot, q, k, w, src, rho))
-            nq = (torch.bincount(sub_id, minlength=n_subs) + 7) // 8
-            grp = sub_id * 8 + rho
-            gcnt = torch.bincount(grp, minlength=n_subs * 8)
-            rank = torch.arange(n, device=dev) - (torch.cumsum(gcnt, 0) - gcnt)[grp]
-            lane = rank * 8 + rho
-            over = rank >= nq[sub_id]
+            # processing order inside a sub-chunk: replicas of one inner operator
+            # together, largest such group first, then (inner, outer, cell)
+            _, pa = torch.sort((q * self.n_outer + k) * cells + cl, stable=True)
+            sub_a, q_a = sub_id[pa], q[pa]
+            key_q = sub_a * n_in + q_a
+            gsz = torch.bincount(key_q)[key_q]
+            _, pb = torch.sort(sub_a * (self.sub_cap + 1) + (self.sub_cap - gsz), stable=True)
+            p2 = pa[pb]
+            sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
+            lane, nq = _pack_quarter_warps(sub_id, q, k, n_subs)
             nslot = nq * 8
             sbase = torch.cumsum(nslot, 0) - nslot
             total = int(nslot.sum())
-            used = torch.zeros(total, dtype=torch.bool, device=dev)
-            used[sbase[sub_id[~over]] + lane[~over]] = True
-            holes = torch.nonzero(~used).squeeze(1)
-            hole_sub = torch.searchsorted(sbase, holes, right=True) - 1
-            hcnt = torch.bincount(hole_sub, minlength=n_subs)
-            hbeg = torch.cumsum(hcnt, 0) - hcnt
-            ov = torch.nonzero(over).squeeze(1)
-            ov_sub = sub_id[ov]
-            ocnt = torch.bincount(ov_sub, minlength=n_subs)
-            orank = torch.arange(ov.numel(), device=dev) - (torch.cumsum(ocnt, 0) - ocnt)[ov_sub]
             dest = sbase[sub_id] + lane
-            dest[ov] = holes[hbeg[ov_sub] + orank]
             pad = torch.ones(total, dtype=torch.bool, device=dev)
             pad[dest] = False
 
@@ -286,6 +272,62 @@ class BrickPlan6:
             ptr(self.uniq), ptr(self.meta), ptr(self.w), self.sub_cap, gz, gy, gx, bz, by, bx, nbz, nby, nbx,
             ptr(self.zero_bricks), int(self.zero_bricks.numel()), ptr(self.cword),
         )
+
+
+def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, n_subs: int):
+    """Lane of every replica inside its sub-chunk, packing ``ceil(n / 8)``
+    quarter-warps of eight lanes first-fit so that the inner operators ``q`` of a
+    quarter-warp are equal or in different bank quads (``q mod 8``), and so are the
+    outer ones ``k``.
+
+    Replicas come grouped by sub-chunk, each group in its processing order; the
+    sub-chunks are packed side by side, one replica of each per step.  A replica
+    goes to the first quarter-warp with a free lane that (1) already reads its
+    inner operator, else (2) has its inner residue free, both with a compatible
+    outer residue, else (3) has a compatible inner residue, else (4) has the
+    fewest lanes taken.  Returns ``(lane, quarter-warps per sub-chunk)``.
+    """
+    dev = sub_id.device
+    n = sub_id.numel()
+    cnt = torch.bincount(sub_id, minlength=n_subs)
+    nq = (cnt + 7) // 8
+    if n == 0:
+        return torch.zeros(0, dtype=torch.int64, device=dev), nq
+    nqw = int(nq.max())
+    step = torch.arange(n, device=dev) - (torch.cumsum(cnt, 0) - cnt)[sub_id]
+    order = torch.sort(step, stable=True)[1]
+    steps = torch.bincount(step)
+    used = torch.zeros(n_subs, nqw, dtype=torch.int64, device=dev)
+    used[torch.arange(nqw, device=dev)[None, :] >= nq[:, None]] = 8  # quarter-warps beyond ceil(n / 8)
+    res_q = torch.full((n_subs, nqw, 8), -1, dtype=torch.int64, device=dev)
+    res_k = torch.full((n_subs, nqw, 8), -1, dtype=torch.int64, device=dev)
+    lane = torch.empty(n, dtype=torch.int64, device=dev)
+    big = nqw + 1
+    col = torch.arange(nqw, device=dev)[None, :]
+    i0 = 0
+    for m in steps.tolist():
+        idx = order[i0:i0 + m]
+        i0 += m
+        sb, qq, kk = sub_id[idx], q[idx], k[idx]
+        cq = res_q[sb[:, None], col, (qq % 8)[:, None]]
+        ck = res_k[sb[:, None], col, (kk % 8)[:, None]]
+        u = used[sb]
+        free = u < 8
+        ok_k = (ck < 0) | (ck == kk[:, None])
+        same_q = cq == qq[:, None]
+        cands = (free & same_q & ok_k, free & (cq < 0) & ok_k, free & ((cq < 0) | same_q))
+        pick = torch.full((m,), big, dtype=torch.int64, device=dev)
+        for c in cands:
+            first = torch.where(c, col, big).min(1).values
+            pick = torch.where(pick == big, first, pick)
+        fewest = torch.where(free, u, 9).argmin(1)
+        pick = torch.where(pick == big, fewest, pick)
+        lane[idx] = pick * 8 + u.gather(1, pick[:, None]).squeeze(1)
+        used[sb, pick] += 1
+        for res, r, v in ((res_q, qq % 8, qq), (res_k, kk % 8, kk)):
+            cur = res[sb, pick, r]
+            res[sb, pick, r] = torch.where(cur < 0, v, cur)
+    return lane, nq
 
 
 def _sm_count(dev) -> int:
