@@ -308,9 +308,11 @@ PGB_API int pgb_grog_degrid_v6(const void* grid, int64_t G, void* out, int64_t N
                                const int32_t* zero_src, int64_t n_zero, void* stream);
 
 /* One-lane-per-replica variants on the v6 plan (C <= 16; plan sub_cap <= 256:
- * one replica per thread of a 256-thread CTA, ordered by (outer, inner, cell)
- * inside each sub-chunk).  inner / outer (forward) and inner_h / outer_h
- * (adjoint): row-major (n, C, C) operators (inner = whole table when
+ * one replica per thread of a 256-thread CTA; any replica order inside a
+ * sub-chunk is correct, the quarter-warp packing of the plan only removes
+ * bank conflicts; entries with meta.x < 0 are padding).  The forward needs
+ * the plan's cell order (cword).  inner / outer (forward) and inner_h /
+ * outer_h (adjoint): row-major (n, C, C) operators (inner = whole table when
  * n_outer == 1).  Same contract as pgb_grog_grid_v6 / pgb_grog_degrid_v6.
  * Shared memory: pgb_grog_v8_smem_bytes(C, cells, n_inner, n_outer, sub_cap). */
 PGB_API size_t pgb_grog_v8_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer,
@@ -319,6 +321,16 @@ PGB_API int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G,
                              int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
                              const pgb_v6_plan* plan, void* stream);
 PGB_API int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h,
+                               int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C, int64_t B,
+                               const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
+                               const int32_t* zero_src, int64_t n_zero, void* stream);
+/* Two threads per replica (512-thread CTA, each thread C / 2 rows of every
+ * product, halves joined with warp shuffles): even C only; otherwise the
+ * same plans, contract and shared memory as the v8 entry points. */
+PGB_API int pgb_grog_grid_v9(const void* data, int64_t N, void* grid, int64_t G, const void* inner,
+                             int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
+                             const pgb_v6_plan* plan, void* stream);
+PGB_API int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h,
                                int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C, int64_t B,
                                const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);

@@ -126,6 +126,8 @@ _SIGS = {
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
     "pgb_grog_grid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
     "pgb_grog_degrid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
+    "pgb_grog_grid_v9": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
+    "pgb_grog_degrid_v9": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
     "pgb_subspace_scatter": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_subspace_gather": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_psf_apply_kk": [_vp, _vp, _i64, _i64, _i64, _i64, _vp],

@@ -452,6 +452,8 @@ class GrogGridder:
                       operator loads are conflict-free or broadcast; the
                       forward sums each cell's replicas without atomics;
       ``"v8pair"``    the v8 adjoint with the v6 forward;
+      ``"v9"``        v8 with two threads per replica (512-thread CTAs, each
+                      thread half the rows of every product), even C;
       ``"v6"``        C <= 16: operator-stationary slots (outer factor rows
                       in registers along sorted runs, inner factor or whole
                       table in shared memory), dynamic work queue;
@@ -469,6 +471,9 @@ class GrogGridder:
     # v8 plans: deal replicas round-robin over inner residues q mod 8 inside
     # outer runs (BrickPlan6 lane_order): fewer shared-memory bank conflicts
     LANE_ORDER_V8 = True
+    # two threads per replica (v9 entry points) by default for even C: measured
+    # slower than one (1.90 / 1.24 against 1.86 / 1.22 ms on the 192^3 kooshball)
+    PAIRS_DEFAULT = False
     # v8 forward: longest run of one cell's replicas summed by one thread
     SEG_LEN_V8 = 24
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
@@ -505,7 +510,11 @@ class GrogGridder:
         chosen = None
         self.sub_cap = None
         self.fwd6 = None  # (brick, sub_cap, factored) of the v6 forward used with the v8 adjoint
-        if mode in (None, "v8", "v8pair") and C <= 16:
+        # v8 family with two threads per replica (v9 entry points)
+        self.pairs = C % 2 == 0 and (mode == "v9" or (mode is None and self.PAIRS_DEFAULT))
+        if mode == "v9" and C % 2:
+            raise ValueError("v9 kernels need an even coil count")
+        if mode in (None, "v8", "v8pair", "v9") and C <= 16:
             n_out_f = int(factors[0].shape[0]) if factors is not None else None
             for sub in (256, 192, 128):
                 for br in cand:
@@ -560,7 +569,7 @@ class GrogGridder:
                     chosen = ("v3", br, True)
                     break
         if chosen is None:
-            if mode in ("v3", "v5", "v6", "v8", "v8pair"):
+            if mode in ("v3", "v5", "v6", "v8", "v8pair", "v9"):
                 raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
             br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
                 (4, 8, 8) if ndim == 3 else (1, 16, 16))
@@ -591,7 +600,8 @@ class GrogGridder:
             self.outer = self.outer_h = None
         self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6 / v8)
         if self.mode == "v8":
-            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap, lane_order=self.LANE_ORDER_V8)
+            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap, lane_order=self.LANE_ORDER_V8,
+                       pair_lanes=self.pairs)
             if self.fwd6 is not None:
                 br6, sub6, _ = self.fwd6
                 self.inner_lc = lane_chunk(self.inner)
@@ -666,7 +676,8 @@ class GrogGridder:
             _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
                       self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
         elif self.mode == "v8":
-            _lib.call("pgb_grog_grid_v8", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
+            _lib.call("pgb_grog_grid_v9" if self.pairs else "pgb_grog_grid_v8", data.data_ptr(), N, out.data_ptr(), G,
+                      self.inner.data_ptr(),
                       self.inner.shape[0], self._outer_ptr(False), self.n_outer, C, B, _ctypes_ref(bp._c), st)
         elif self.mode == "v6":
             olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
@@ -690,7 +701,8 @@ class GrogGridder:
         zs = bp.zero_src.data_ptr() if bp.zero_src.numel() else None
         if self.mode == "v8":
             sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
-            _lib.call("pgb_grog_degrid_v8", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
+            _lib.call("pgb_grog_degrid_v9" if self.pairs else "pgb_grog_degrid_v8", grid.data_ptr(), G,
+                      out.data_ptr(), N, self.inner_h.data_ptr(),
                       self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,
                       _ctypes_ref(bp._c), sec, zs, int(bp.zero_src.numel()), st)
         elif self.mode == "v6":

@@ -37,7 +37,8 @@ class BrickPlan6:
 
     Arrays (all on the plan's device unless noted):
       ``subs``   int32 (n_subs, 4) ``{rep_begin, rep_end, uniq_begin, uniq_end}``
-      ``uniq``   int32 source sample of every staging slot
+      ``uniq``   int32 source sample of every staging slot (ascending inside a
+                 sub-chunk: neighbouring threads stage neighbouring samples)
       ``meta``   int32 (n_valid, 2) ``{cell | slot << 16, inner | outer << 16}``
       ``w``      float32 replica weight
       ``sd`` / ``si`` / ``cta_ptr``  per-CTA sub-chunk streams: descriptor,
@@ -71,6 +72,7 @@ class BrickPlan6:
         lane_order: bool = False,
         cell_order: bool = False,
         seg_len: int = 8,
+        pair_lanes: bool = False,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -135,11 +137,11 @@ class BrickPlan6:
         slot = inv - ubeg[sub_id]
 
         # (2) order inside a sub-chunk: (outer, inner, cell).  With lane_order
-        # (one replica per lane) the sub-chunk is laid out in whole
-        # quarter-warps whose eight lanes read inner operators in different bank
-        # quads (inner operator q starts in quad q mod 8) or the same operator,
-        # and likewise outer ones (_pack_quarter_warps); the lanes left free are
-        # padding entries (meta -1, weight 0), fewer than eight per sub-chunk.
+        # (one replica per lane, or per lane pair with pair_lanes) the sub-chunk
+        # is laid out in whole quarter-warps whose lanes read inner operators in
+        # different bank quads or the same operator, and likewise outer ones
+        # (_pack_quarter_warps); the places left free are padding entries
+        # (meta -1, weight 0), fewer than one quarter-warp per sub-chunk.
         n_in = int(q.max()) + 1 if n else 1
         pad = torch.zeros(0, dtype=torch.bool, device=dev)
         if lane_order and n:
@@ -152,8 +154,9 @@ class BrickPlan6:
             _, pb = torch.sort(sub_a * (self.sub_cap + 1) + (self.sub_cap - gsz), stable=True)
             p2 = pa[pb]
             sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
-            lane, nq = _pack_quarter_warps(sub_id, q, k, n_subs)
-            nslot = nq * 8
+            per = 4 if pair_lanes else 8  # replicas per quarter-warp
+            lane, nq = _pack_quarter_warps(sub_id, q, k, n_subs, per)
+            nslot = nq * per
             sbase = torch.cumsum(nslot, 0) - nslot
             total = int(nslot.sum())
             dest = sbase[sub_id] + lane
@@ -274,11 +277,13 @@ class BrickPlan6:
         )
 
 
-def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, n_subs: int):
-    """Lane of every replica inside its sub-chunk, packing ``ceil(n / 8)``
-    quarter-warps of eight lanes first-fit so that the inner operators ``q`` of a
-    quarter-warp are equal or in different bank quads (``q mod 8``), and so are the
-    outer ones ``k``.
+def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, n_subs: int, per: int = 8):
+    """Position of every replica inside its sub-chunk, packing ``ceil(n / per)``
+    quarter-warps of ``per`` replicas first-fit so that the inner operators ``q``
+    of a quarter-warp are equal or in different bank-quad classes, and so are the
+    outer ones ``k``.  ``per = 8``: one lane per replica, operator q starts in
+    quad q mod 8.  ``per = 4``: two lanes per replica reading rows 0..C/2-1 and
+    C/2..C-1 (4 quads apart when C = 12, mod 8), classes q mod 4.
 
     Replicas come grouped by sub-chunk, each group in its processing order; the
     sub-chunks are packed side by side, one replica of each per step.  A replica
@@ -290,7 +295,8 @@ def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, 
     dev = sub_id.device
     n = sub_id.numel()
     cnt = torch.bincount(sub_id, minlength=n_subs)
-    nq = (cnt + 7) // 8
+    nq = (cnt + per - 1) // per
+    nres = per
     if n == 0:
         return torch.zeros(0, dtype=torch.int64, device=dev), nq
     nqw = int(nq.max())
@@ -298,9 +304,9 @@ def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, 
     order = torch.sort(step, stable=True)[1]
     steps = torch.bincount(step)
     used = torch.zeros(n_subs, nqw, dtype=torch.int64, device=dev)
-    used[torch.arange(nqw, device=dev)[None, :] >= nq[:, None]] = 8  # quarter-warps beyond ceil(n / 8)
-    res_q = torch.full((n_subs, nqw, 8), -1, dtype=torch.int64, device=dev)
-    res_k = torch.full((n_subs, nqw, 8), -1, dtype=torch.int64, device=dev)
+    used[torch.arange(nqw, device=dev)[None, :] >= nq[:, None]] = per  # quarter-warps beyond ceil(n / per)
+    res_q = torch.full((n_subs, nqw, nres), -1, dtype=torch.int64, device=dev)
+    res_k = torch.full((n_subs, nqw, nres), -1, dtype=torch.int64, device=dev)
     lane = torch.empty(n, dtype=torch.int64, device=dev)
     big = nqw + 1
     col = torch.arange(nqw, device=dev)[None, :]
@@ -309,10 +315,10 @@ def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, 
         idx = order[i0:i0 + m]
         i0 += m
         sb, qq, kk = sub_id[idx], q[idx], k[idx]
-        cq = res_q[sb[:, None], col, (qq % 8)[:, None]]
-        ck = res_k[sb[:, None], col, (kk % 8)[:, None]]
+        cq = res_q[sb[:, None], col, (qq % nres)[:, None]]
+        ck = res_k[sb[:, None], col, (kk % nres)[:, None]]
         u = used[sb]
-        free = u < 8
+        free = u < per
         ok_k = (ck < 0) | (ck == kk[:, None])
         same_q = cq == qq[:, None]
         cands = (free & same_q & ok_k, free & (cq < 0) & ok_k, free & ((cq < 0) | same_q))
@@ -320,11 +326,11 @@ def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, 
         for c in cands:
             first = torch.where(c, col, big).min(1).values
             pick = torch.where(pick == big, first, pick)
-        fewest = torch.where(free, u, 9).argmin(1)
+        fewest = torch.where(free, u, per + 1).argmin(1)
         pick = torch.where(pick == big, fewest, pick)
-        lane[idx] = pick * 8 + u.gather(1, pick[:, None]).squeeze(1)
+        lane[idx] = pick * per + u.gather(1, pick[:, None]).squeeze(1)
         used[sb, pick] += 1
-        for res, r, v in ((res_q, qq % 8, qq), (res_k, kk % 8, kk)):
+        for res, r, v in ((res_q, qq % nres, qq), (res_k, kk % nres, kk)):
             cur = res[sb, pick, r]
             res[sb, pick, r] = torch.where(cur < 0, v, cur)
     return lane, nq

@@ -90,20 +90,21 @@ __device__ __forceinline__ void wait8() {
 }
 
 // Copy (n, C, C) row-major operators into the padded shared-memory layout.
-template <int C>
+template <int C, int NT>
 __device__ __forceinline__ void stage_ops8(float2* __restrict__ dst, const float2* __restrict__ src, int n) {
   constexpr int per = C * C;
-  for (int t = threadIdx.x; t < n * per; t += kT8) {
+  for (int t = threadIdx.x; t < n * per; t += NT) {
     const int m = t / per;
     dst[m * Pad8<C>::OPS + (t - m * per)] = __ldg(src + t);
   }
 }
 
-// y = M x for one row-major C x C operator in shared memory.
-template <int C>
-__device__ __forceinline__ void matvec8(const float2* __restrict__ M, const float2 (&x)[C], float2 (&y)[C]) {
+// y = rows 0..NR-1 of M times x, M a row-major C x C operator (or the NR-row
+// slice of one) in shared memory.
+template <int C, int NR = C>
+__device__ __forceinline__ void matvec8(const float2* __restrict__ M, const float2 (&x)[C], float2 (&y)[NR]) {
 #pragma unroll
-  for (int r = 0; r < C; ++r) {
+  for (int r = 0; r < NR; ++r) {
     float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
     const float2* row = M + r * C;
     if constexpr (C % 2 == 0) {
@@ -118,6 +119,18 @@ __device__ __forceinline__ void matvec8(const float2* __restrict__ M, const floa
       for (int j = 0; j < C; ++j) cfma((j & 1) ? a1 : a0, row[j], x[j]);
     }
     y[r] = make_float2(a0.x + a1.x, a0.y + a1.y);
+  }
+}
+
+// Two threads per replica (lanes 2i, 2i + 1): each computed H = C / 2 rows of
+// a product; returns the full vector in row order on both.
+template <int C>
+__device__ __forceinline__ void join_halves8(const float2 (&mine)[C / 2], int h, float2 (&full)[C]) {
+#pragma unroll
+  for (int i = 0; i < C / 2; ++i) {
+    const float2 o = make_float2(__shfl_xor_sync(0xffffffffu, mine[i].x, 1), __shfl_xor_sync(0xffffffffu, mine[i].y, 1));
+    full[i] = h ? o : mine[i];
+    full[C / 2 + i] = h ? mine[i] : o;
   }
 }
 
@@ -161,8 +174,7 @@ __device__ __forceinline__ int nrp8(int4 d, int cap) { return min(max(d.y - d.x,
 
 // This lane's replica of sub-chunk d: metadata and weight (zeros past the end).
 __device__ __forceinline__ void ld_rep8(const int2* __restrict__ meta, const float* __restrict__ wts, int4 d,
-                                        int cap, int2& m, float& w) {
-  const int t = threadIdx.x;
+                                        int cap, int t, int2& m, float& w) {
   if (t < nrp8(d, cap)) {
     m = __ldg(meta + d.x + t);
     w = __ldg(wts + d.x + t);
@@ -190,8 +202,8 @@ __device__ __forceinline__ void stage_x8(const float2* __restrict__ dat, int64_t
   }
 }
 
-template <int C, bool OUTER>
-__global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
+template <int C, bool OUTER, int NT>
+__global__ void __launch_bounds__(NT, 1) grog_grid_v8_kernel(
     const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G,
     const float2* __restrict__ inner, int n_inner, const float2* __restrict__ outer, int n_outer,
     const int4* __restrict__ sd, const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr,
@@ -199,6 +211,9 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
     const int32_t* __restrict__ cword, int cap, Geom8 geom) {
   extern __shared__ float4 smem4[];
   constexpr int OPS = Pad8<C>::OPS;
+  constexpr bool PAIR = NT > kT8;  // two threads per replica, H rows of each product
+  constexpr int H = PAIR ? C / 2 : C;
+  static_assert(!PAIR || (C % 2 == 0 && NT == 2 * kT8), "thread pairs need an even coil count");
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;  // block-uniform
   const int cells = geom.bz * geom.by * geom.bx;
@@ -216,6 +231,8 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
   const float2* dat = data + static_cast<int64_t>(b) * C * N;
   float2* grd = grid + static_cast<int64_t>(b) * C * G;
   const int tid = threadIdx.x;
+  const int rr = PAIR ? tid >> 1 : tid;  // this thread's replica in the sub-chunk
+  const int h = PAIR ? tid & 1 : 0;      // and which half of the rows it computes
 
   Stream8 st;
   st.init(sd, si, p0, p1);
@@ -227,15 +244,15 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
   }
   int2 m0, m1;
   float w0, w1;
-  ld_rep8(meta, wts, st.d0, cap, m0, w0);
-  ld_rep8(meta, wts, st.d1, cap, m1, w1);
+  ld_rep8(meta, wts, st.d0, cap, rr, m0, w0);
+  ld_rep8(meta, wts, st.d1, cap, rr, m1, w1);
   auto ld_cw = [&](int4 d, bool valid) -> int32_t {
     return (valid && tid < nrp8(d, cap)) ? __ldg(cword + d.x + tid) : 0;
   };
   int32_t c0 = ld_cw(st.d0, true), c1 = ld_cw(st.d1, st.p + 1 < p1);
-  stage_ops8<C>(tin, inner, n_inner);
-  if (OUTER) stage_ops8<C>(tout, outer, n_outer);
-  for (int t = tid; t < 2 * C * TS; t += kT8) tre[t] = 0.f;
+  stage_ops8<C, NT>(tin, inner, n_inner);
+  if (OUTER) stage_ops8<C, NT>(tout, outer, n_outer);
+  for (int t = tid; t < 2 * C * TS; t += NT) tre[t] = 0.f;
 
   int buf = 0;
   while (true) {
@@ -251,7 +268,7 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
     const int u2 = ld_uniq8(uniq, st.d2, cap, st.p + 2 < p1);
     int2 m2;
     float w2;
-    ld_rep8(meta, wts, st.p + 2 < p1 ? st.d2 : make_int4(0, 0, 0, 0), cap, m2, w2);
+    ld_rep8(meta, wts, st.p + 2 < p1 ? st.d2 : make_int4(0, 0, 0, 0), cap, rr, m2, w2);
     const int32_t c2 = ld_cw(st.d2, st.p + 2 < p1);
     __syncthreads();  // staging buffer `buf` complete; tile zeroed
     {
@@ -263,24 +280,41 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
       const int k = static_cast<int>(static_cast<unsigned>(m0.y) >> 16);
       const bool on = m0.x >= 0 && cell < cells && sl < nu && q < n_inner && (OUTER ? k < n_outer : k == 0);
       float2* xs = xs0 + buf * C * cap;
-      float2 x[C], u[C];
-      if (on) {
+      float2 y[H];
+      if constexpr (PAIR) {
+        // both threads of a pair run every step (the halves are exchanged with
+        // shuffles); an idle pair works on operator 0 and slot 0, writes zeros
+        const int slc = on ? sl : 0, qc = on ? q : 0, kc = on ? k : 0;
+        float2 x[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) x[c] = xs[c * cap + slc];
+        if constexpr (OUTER) {
+          float2 uh[H], u[C];
+          matvec8<C, H>(tin + qc * OPS + h * H * C, x, uh);
+          join_halves8<C>(uh, h, u);
+          matvec8<C, H>(tout + kc * OPS + h * H * C, u, y);
+        } else {
+          matvec8<C, H>(tin + qc * OPS + h * H * C, x, y);
+        }
+      } else if (on) {
+        float2 x[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) x[c] = xs[c * cap + sl];
-        matvec8<C>(tin + q * OPS, x, u);
         if constexpr (OUTER) {
-          matvec8<C>(tout + k * OPS, u, x);
-#pragma unroll
-          for (int c = 0; c < C; ++c) u[c] = x[c];
+          float2 u[C];
+          matvec8<C>(tin + q * OPS, x, u);
+          matvec8<C, H>(tout + k * OPS, u, y);
+        } else {
+          matvec8<C, H>(tin + q * OPS, x, y);
         }
       }
       __syncthreads();  // every lane has read its staged coils: the buffer takes the results
-      if (tid < nr) {
+      if (rr < nr) {
 #pragma unroll
-        for (int c = 0; c < C; ++c)
-          xs[c * cap + tid] = on ? make_float2(w0 * u[c].x, w0 * u[c].y) : make_float2(0.f, 0.f);
-        cws[tid] = c0;
+        for (int i = 0; i < H; ++i)
+          xs[(h * H + i) * cap + rr] = on ? make_float2(w0 * y[i].x, w0 * y[i].y) : make_float2(0.f, 0.f);
       }
+      if (tid < nr) cws[tid] = c0;
       __syncthreads();
       // one owner per segment (the head of at most a few entries of one cell
       // in cell order) sums the segment's results and updates the tile; only
@@ -329,7 +363,7 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
       int z0, y0, x0;
       origin8(geom, st.i0.x, z0, y0, x0);
       const bool split = (st.i0.y & kSplit8) != 0;
-      for (int t = tid; t < C * cells; t += kT8) {
+      for (int t = tid; t < C * cells; t += NT) {
         const int c = t / cells;
         const int cl = t - c * cells;
         const float2 v = make_float2(tre[c * TS + cl], tim[c * TS + cl]);
@@ -361,8 +395,8 @@ __global__ void __launch_bounds__(kT8, 1) grog_grid_v8_kernel(
   }
 }
 
-template <int C, bool OUTER, bool ACC>
-__global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
+template <int C, bool OUTER, bool ACC, int NT>
+__global__ void __launch_bounds__(NT, 1) grog_degrid_v8_kernel(
     const float2* __restrict__ grid, int64_t G, float2* __restrict__ out, int64_t N,
     const float2* __restrict__ inner_h, int n_inner, const float2* __restrict__ outer_h, int n_outer,
     const int4* __restrict__ sd, const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr,
@@ -370,6 +404,9 @@ __global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
     Geom8 geom) {
   extern __shared__ float4 smem4[];
   constexpr int OPS = Pad8<C>::OPS;
+  constexpr bool PAIR = NT > kT8;  // two threads per replica, H rows of each product
+  constexpr int H = PAIR ? C / 2 : C;
+  static_assert(!PAIR || (C % 2 == 0 && NT == 2 * kT8), "thread pairs need an even coil count");
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;
   const int cells = geom.bz * geom.by * geom.bx;
@@ -383,11 +420,13 @@ __global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
   const float2* grd = grid + static_cast<int64_t>(b) * C * G;
   float2* o = out + static_cast<int64_t>(b) * C * N;
   const int tid = threadIdx.x;
+  const int rr = PAIR ? tid >> 1 : tid;  // this thread's replica in the sub-chunk
+  const int h = PAIR ? tid & 1 : 0;      // and which half of the rows it computes
 
   auto issue_tile = [&](int brick, float2* tl) {
     int z0, y0, x0;
     origin8(geom, brick, z0, y0, x0);
-    for (int t = tid; t < C * cells; t += kT8) {
+    for (int t = tid; t < C * cells; t += NT) {
       const int c = t / cells;
       const int cl = t - c * cells;
       int64_t flat;
@@ -401,15 +440,15 @@ __global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
   int par = 0;  // tile buffer of the current brick item
   issue_tile(st.i0.x, tiles);
   commit8();
-  stage_ops8<C>(tin, inner_h, n_inner);
-  if (OUTER) stage_ops8<C>(tout, outer_h, n_outer);
-  for (int t = tid; t < C * cap; t += kT8) res[t] = make_float2(0.f, 0.f);
+  stage_ops8<C, NT>(tin, inner_h, n_inner);
+  if (OUTER) stage_ops8<C, NT>(tout, outer_h, n_outer);
+  for (int t = tid; t < C * cap; t += NT) res[t] = make_float2(0.f, 0.f);
   int u0 = ld_uniq8(uniq, st.d0, cap, true);
   int u1 = ld_uniq8(uniq, st.d1, cap, st.p + 1 < p1);
   int2 m0, m1;
   float w0, w1;
-  ld_rep8(meta, wts, st.d0, cap, m0, w0);
-  ld_rep8(meta, wts, st.d1, cap, m1, w1);
+  ld_rep8(meta, wts, st.d0, cap, rr, m0, w0);
+  ld_rep8(meta, wts, st.d1, cap, rr, m1, w1);
 
   while (true) {
     const bool more = st.p + 1 < p1;
@@ -424,7 +463,7 @@ __global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
     const int u2 = ld_uniq8(uniq, st.d2, cap, st.p + 2 < p1);
     int2 m2;
     float w2;
-    ld_rep8(meta, wts, st.p + 2 < p1 ? st.d2 : make_int4(0, 0, 0, 0), cap, m2, w2);
+    ld_rep8(meta, wts, st.p + 2 < p1 ? st.d2 : make_int4(0, 0, 0, 0), cap, rr, m2, w2);
     __syncthreads();  // tile of this brick complete; previous results flushed and cleared
     {
       const int nu = nsl8(st.d0, cap);
@@ -433,7 +472,39 @@ __global__ void __launch_bounds__(kT8, 1) grog_degrid_v8_kernel(
       const int q = m0.y & 0xFFFF;
       const int k = static_cast<int>(static_cast<unsigned>(m0.y) >> 16);
       const bool on = m0.x >= 0 && cell < cells && sl < nu && q < n_inner && (OUTER ? k < n_outer : k == 0);
-      if (on) {
+      if constexpr (PAIR) {
+        // both threads of a pair run every step (the halves are exchanged with
+        // shuffles); an idle pair works on cell 0 and operator 0, writes nothing
+        const int cc = on ? cell : 0, qc = on ? q : 0, kc = on ? k : 0;
+        const float2* gt = tiles + par * lay.tile_sz + cc * C;
+        float2 g[C], r[H];
+#pragma unroll
+        for (int c = 0; c < C; c += 2) {
+          const float4 v = *reinterpret_cast<const float4*>(gt + c);
+          g[c] = make_float2(v.x, v.y);
+          g[c + 1] = make_float2(v.z, v.w);
+        }
+        if constexpr (OUTER) {
+          float2 yh[H], y[C];
+          matvec8<C, H>(tout + kc * OPS + h * H * C, g, yh);
+          join_halves8<C>(yh, h, y);
+          matvec8<C, H>(tin + qc * OPS + h * H * C, y, r);
+        } else {
+          matvec8<C, H>(tin + qc * OPS + h * H * C, g, r);
+        }
+        if (on) {
+#pragma unroll
+          for (int i = 0; i < H; ++i) {
+            float2* dst = res + (h * H + i) * cap + sl;
+            if (ACC) {
+              atomicAdd(&dst->x, w0 * r[i].x);
+              atomicAdd(&dst->y, w0 * r[i].y);
+            } else {
+              *dst = make_float2(w0 * r[i].x, w0 * r[i].y);
+            }
+          }
+        }
+      } else if (on) {
         const float2* gt = tiles + par * lay.tile_sz + cell * C;
         float2 g[C], y[C];
         if constexpr (C % 2 == 0) {
@@ -580,92 +651,124 @@ size_t pgb_grog_v8_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t
   return a > b ? a : b;
 }
 
-int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const void* inner, int64_t n_inner,
-                     const void* outer, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* plan,
-                     void* stream) {
-  clear_error();
+}  // extern "C"
+
+namespace {
+
+// Shared by the one-thread (v8, NT = 256) and two-thread-per-replica (v9,
+// NT = 512, even C) launches; `who` names the entry point in errors.
+int grid_v8_launch(int nt, const char* who, const void* data, int64_t N, void* grid, int64_t G,
+                   const void* inner, int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
+                   const pgb_v6_plan* plan, void* stream) {
   Geom8 geom;
-  int st = v8_geom(plan, geom, "grog_grid_v8");
+  int st = v8_geom(plan, geom, who);
   if (st) return st;
-  PGB_REQUIRE(C >= 1 && C <= 16, PGB_ERR_UNSUPPORTED, "grog_grid_v8: ncoils must be 1..16, got %lld",
-              (long long)C);
+  PGB_REQUIRE(C >= 1 && C <= 16 && (nt == kT8 || C % 2 == 0), PGB_ERR_UNSUPPORTED,
+              "%s: ncoils must be 1..16 (even for thread pairs), got %lld", who, (long long)C);
   PGB_REQUIRE(N >= 0 && N < (int64_t(1) << 31) && B >= 0 && B <= 65535 && n_inner >= 1 && n_inner <= 65535 &&
                   n_outer >= 1 && n_outer <= 65535,
-              PGB_ERR_RANGE, "grog_grid_v8: invalid N/B/table sizes");
-  PGB_REQUIRE(n_outer == 1 || outer != nullptr, PGB_ERR_INVALID, "grog_grid_v8: null outer table");
+              PGB_ERR_RANGE, "%s: invalid N/B/table sizes", who);
+  PGB_REQUIRE(n_outer == 1 || outer != nullptr, PGB_ERR_INVALID, "%s: null outer table", who);
   PGB_REQUIRE(G == static_cast<int64_t>(plan->gz) * plan->gy * plan->gx, PGB_ERR_INVALID,
-              "grog_grid_v8: G does not match the plan grid");
+              "%s: G does not match the plan grid", who);
   if (B == 0 || G == 0) return PGB_OK;
-  PGB_REQUIRE(grid && inner && (data || N == 0), PGB_ERR_INVALID, "grog_grid_v8: null pointer");
+  PGB_REQUIRE(grid && inner && (data || N == 0), PGB_ERR_INVALID, "%s: null pointer", who);
   const int cells = plan->bz * plan->by * plan->bx;
   const size_t smem = v8_smem_c(C, cells, n_inner, n_outer, plan->sub_cap, true);
   PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED,
-              "grog_grid_v8: tables + tile + staging need %zu B of shared memory", smem);
+              "%s: tables + tile + staging need %zu B of shared memory", who, smem);
   cudaStream_t s = as_stream(stream);
   if (plan->n_zero_bricks > 0) {
-    PGB_REQUIRE(plan->zero_bricks != nullptr, PGB_ERR_INVALID, "grog_grid_v8: null zero-brick list");
+    PGB_REQUIRE(plan->zero_bricks != nullptr, PGB_ERR_INVALID, "%s: null zero-brick list", who);
     const int64_t tot = static_cast<int64_t>(plan->n_zero_bricks) * cells;
     zero_bricks_v8<<<grid_for(tot, 256, 148 * 16), 256, 0, s>>>(static_cast<float2*>(grid), G, static_cast<int>(C),
                                                                static_cast<int>(B), plan->zero_bricks,
                                                                plan->n_zero_bricks, geom);
-    PGB_LAUNCH_CHECK("grog_grid_v8(zero bricks)");
+    PGB_LAUNCH_CHECK(who);
   }
   if (plan->n_cta == 0) return PGB_OK;
-  PGB_REQUIRE(plan->cword != nullptr, PGB_ERR_INVALID, "grog_grid_v8: the plan has no cell order (cword)");
+  PGB_REQUIRE(plan->cword != nullptr, PGB_ERR_INVALID, "%s: the plan has no cell order (cword)", who);
   const bool has_outer = n_outer > 1;
   dim3 grd(plan->n_cta, static_cast<unsigned>(B));
   switch (C) {
-#define X(CC)                                                                                               \
-  case CC: {                                                                                                \
-    auto k = has_outer ? grog_grid_v8_kernel<CC, true> : grog_grid_v8_kernel<CC, false>;                    \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                        \
-    k<<<grd, kT8, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,             \
-                             static_cast<const float2*>(inner), static_cast<int>(n_inner),                  \
-                             static_cast<const float2*>(outer), static_cast<int>(n_outer),                  \
-                             reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si), \
-                             plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,  \
-                             plan->cword, plan->sub_cap, geom);                                             \
+#define X(CC)                                                                                                 \
+  case CC: {                                                                                                  \
+    auto k = has_outer ? grog_grid_v8_kernel<CC, true, kT8> : grog_grid_v8_kernel<CC, false, kT8>;            \
+    if constexpr (CC % 2 == 0) {                                                                              \
+      if (nt != kT8) k = has_outer ? grog_grid_v8_kernel<CC, true, 2 * kT8> : grog_grid_v8_kernel<CC, false, 2 * kT8>; \
+    }                                                                                                         \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                          \
+    k<<<grd, nt, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,                \
+                            static_cast<const float2*>(inner), static_cast<int>(n_inner),                     \
+                            static_cast<const float2*>(outer), static_cast<int>(n_outer),                     \
+                            reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),  \
+                            plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,     \
+                            plan->cword, plan->sub_cap, geom);                                                \
   } break;
     PGB8_FOR_EACH_C(X)
 #undef X
     default:
       break;
   }
-  PGB_LAUNCH_CHECK("grog_grid_v8");
+  PGB_LAUNCH_CHECK(who);
   return PGB_OK;
 }
 
-int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h, int64_t n_inner,
-                       const void* outer_h, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* primary,
-                       const pgb_v6_plan* secondary, const int32_t* zero_src, int64_t n_zero, void* stream) {
+}  // namespace
+
+extern "C" {
+
+int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const void* inner, int64_t n_inner,
+                     const void* outer, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* plan,
+                     void* stream) {
   clear_error();
+  return grid_v8_launch(kT8, "grog_grid_v8", data, N, grid, G, inner, n_inner, outer, n_outer, C, B, plan, stream);
+}
+
+int pgb_grog_grid_v9(const void* data, int64_t N, void* grid, int64_t G, const void* inner, int64_t n_inner,
+                     const void* outer, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* plan,
+                     void* stream) {
+  clear_error();
+  return grid_v8_launch(2 * kT8, "grog_grid_v9", data, N, grid, G, inner, n_inner, outer, n_outer, C, B, plan,
+                        stream);
+}
+
+
+}  // extern "C"
+
+namespace {
+
+int degrid_v8_launch(int nt, const char* who, const void* grid, int64_t G, void* out, int64_t N,
+                     const void* inner_h, int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C,
+                     int64_t B, const pgb_v6_plan* primary, const pgb_v6_plan* secondary, const int32_t* zero_src,
+                     int64_t n_zero, void* stream) {
   Geom8 geom;
-  int st = v8_geom(primary, geom, "grog_degrid_v8");
+  int st = v8_geom(primary, geom, who);
   if (st) return st;
   if (secondary != nullptr) {
     Geom8 g2;
-    st = v8_geom(secondary, g2, "grog_degrid_v8(secondary)");
+    st = v8_geom(secondary, g2, who);
     if (st) return st;
     PGB_REQUIRE(secondary->bz == primary->bz && secondary->by == primary->by && secondary->bx == primary->bx &&
                     secondary->gz == primary->gz && secondary->gy == primary->gy && secondary->gx == primary->gx,
-                PGB_ERR_INVALID, "grog_degrid_v8: primary and secondary plans differ in geometry");
+                PGB_ERR_INVALID, "%s: primary and secondary plans differ in geometry", who);
   }
-  PGB_REQUIRE(C >= 1 && C <= 16, PGB_ERR_UNSUPPORTED, "grog_degrid_v8: ncoils must be 1..16, got %lld",
-              (long long)C);
+  PGB_REQUIRE(C >= 1 && C <= 16 && (nt == kT8 || C % 2 == 0), PGB_ERR_UNSUPPORTED,
+              "%s: ncoils must be 1..16 (even for thread pairs), got %lld", who, (long long)C);
   PGB_REQUIRE(N >= 0 && N < (int64_t(1) << 31) && B >= 0 && B <= 65535 && n_inner >= 1 && n_inner <= 65535 &&
                   n_outer >= 1 && n_outer <= 65535 && n_zero >= 0,
-              PGB_ERR_RANGE, "grog_degrid_v8: invalid N/B/table sizes");
-  PGB_REQUIRE(n_outer == 1 || outer_h != nullptr, PGB_ERR_INVALID, "grog_degrid_v8: null outer table");
+              PGB_ERR_RANGE, "%s: invalid N/B/table sizes", who);
+  PGB_REQUIRE(n_outer == 1 || outer_h != nullptr, PGB_ERR_INVALID, "%s: null outer table", who);
   PGB_REQUIRE(G == static_cast<int64_t>(primary->gz) * primary->gy * primary->gx, PGB_ERR_INVALID,
-              "grog_degrid_v8: G does not match the plan grid");
+              "%s: G does not match the plan grid", who);
   if (B == 0 || N == 0) return PGB_OK;
-  PGB_REQUIRE(out && inner_h && (grid || G == 0), PGB_ERR_INVALID, "grog_degrid_v8: null pointer");
+  PGB_REQUIRE(out && inner_h && (grid || G == 0), PGB_ERR_INVALID, "%s: null pointer", who);
   cudaStream_t s = as_stream(stream);
   if (n_zero > 0) {
-    PGB_REQUIRE(zero_src != nullptr, PGB_ERR_INVALID, "grog_degrid_v8: null zero list");
+    PGB_REQUIRE(zero_src != nullptr, PGB_ERR_INVALID, "%s: null zero list", who);
     zero_samples_v8<<<grid_for(n_zero * C * B, 256, 148 * 8), 256, 0, s>>>(
         static_cast<float2*>(out), N, static_cast<int>(C), static_cast<int>(B), zero_src, n_zero);
-    PGB_LAUNCH_CHECK("grog_degrid_v8(zero samples)");
+    PGB_LAUNCH_CHECK(who);
   }
   const bool has_outer = n_outer > 1;
   const int cells = primary->bz * primary->by * primary->bx;
@@ -674,29 +777,54 @@ int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const 
     if (p == nullptr || p->n_cta == 0) continue;
     const size_t smem = v8_smem_c(C, cells, n_inner, n_outer, p->sub_cap, false);
     PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED,
-                "grog_degrid_v8: tables + tiles + results need %zu B of shared memory", smem);
+                "%s: tables + tiles + results need %zu B of shared memory", who, smem);
     dim3 grd(p->n_cta, static_cast<unsigned>(B));
     switch (C) {
 #define X(CC)                                                                                                 \
   case CC: {                                                                                                  \
-    auto k = has_outer ? (pass ? grog_degrid_v8_kernel<CC, true, true> : grog_degrid_v8_kernel<CC, true, false>) \
-                       : (pass ? grog_degrid_v8_kernel<CC, false, true> : grog_degrid_v8_kernel<CC, false, false>); \
+    auto k = has_outer ? (pass ? grog_degrid_v8_kernel<CC, true, true, kT8> : grog_degrid_v8_kernel<CC, true, false, kT8>) \
+                       : (pass ? grog_degrid_v8_kernel<CC, false, true, kT8> : grog_degrid_v8_kernel<CC, false, false, kT8>); \
+    if constexpr (CC % 2 == 0) {                                                                              \
+      if (nt != kT8)                                                                                          \
+        k = has_outer ? (pass ? grog_degrid_v8_kernel<CC, true, true, 2 * kT8> : grog_degrid_v8_kernel<CC, true, false, 2 * kT8>) \
+                      : (pass ? grog_degrid_v8_kernel<CC, false, true, 2 * kT8> : grog_degrid_v8_kernel<CC, false, false, 2 * kT8>); \
+    }                                                                                                         \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                          \
-    k<<<grd, kT8, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                \
-                             static_cast<const float2*>(inner_h), static_cast<int>(n_inner),                  \
-                             static_cast<const float2*>(outer_h), static_cast<int>(n_outer),                  \
-                             reinterpret_cast<const int4*>(p->sd), reinterpret_cast<const int2*>(p->si),      \
-                             p->cta_ptr, p->uniq, reinterpret_cast<const int2*>(p->meta), p->w, p->sub_cap,   \
-                             geom);                                                                           \
+    k<<<grd, nt, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                 \
+                            static_cast<const float2*>(inner_h), static_cast<int>(n_inner),                   \
+                            static_cast<const float2*>(outer_h), static_cast<int>(n_outer),                   \
+                            reinterpret_cast<const int4*>(p->sd), reinterpret_cast<const int2*>(p->si),       \
+                            p->cta_ptr, p->uniq, reinterpret_cast<const int2*>(p->meta), p->w, p->sub_cap,    \
+                            geom);                                                                            \
   } break;
       PGB8_FOR_EACH_C(X)
 #undef X
       default:
         break;
     }
-    PGB_LAUNCH_CHECK("grog_degrid_v8");
+    PGB_LAUNCH_CHECK(who);
   }
   return PGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h, int64_t n_inner,
+                       const void* outer_h, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* primary,
+                       const pgb_v6_plan* secondary, const int32_t* zero_src, int64_t n_zero, void* stream) {
+  clear_error();
+  return degrid_v8_launch(kT8, "grog_degrid_v8", grid, G, out, N, inner_h, n_inner, outer_h, n_outer, C, B, primary,
+                          secondary, zero_src, n_zero, stream);
+}
+
+int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h, int64_t n_inner,
+                       const void* outer_h, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* primary,
+                       const pgb_v6_plan* secondary, const int32_t* zero_src, int64_t n_zero, void* stream) {
+  clear_error();
+  return degrid_v8_launch(2 * kT8, "grog_degrid_v9", grid, G, out, N, inner_h, n_inner, outer_h, n_outer, C, B,
+                          primary, secondary, zero_src, n_zero, stream);
 }
 
 }  // extern "C"

@@ -238,17 +238,59 @@ def test_brick_plan6_lane_order_residue_columns():
 
     ca = cb = 0
     wa, wb = a.w.numpy(), b.w.numpy()
-    for (r0, r1, _, _), (t0, t1, _, _) in zip(a.subs.numpy(), b.subs.numpy()):
+    for (r0, r1, u0a, _), (t0, t1, u0b, _) in zip(a.subs.numpy(), b.subs.numpy()):
         ma = a.meta.numpy()[r0:r1].astype(np.int64)
         mb = b.meta.numpy()[t0:t1].astype(np.int64)
         real = mb[:, 0] >= 0
         # whole quarter-warps, fewer than eight padding entries, the same replicas
         assert (t1 - t0) % 8 == 0 and t1 - t0 <= 256 and (t1 - t0) - (r1 - r0) < 8
-        assert sorted(map(tuple, ma.tolist())) == sorted(map(tuple, mb[real].tolist()))
-        assert sorted(wa[r0:r1].tolist()) == sorted(wb[t0:t1][real].tolist())
+        # the same replicas: (cell, inner | outer << 16, sample, weight)
+        ua_, ub_ = a.uniq.numpy(), b.uniq.numpy()
+        sa = ua_[u0a + (ma[:, 0] >> 16)]
+        sbm = ub_[u0b + (mb[real, 0] >> 16)]
+        ra = sorted(zip((ma[:, 0] & 0xFFFF).tolist(), ma[:, 1].tolist(), sa.tolist(), wa[r0:r1].tolist()))
+        rb = sorted(zip((mb[real, 0] & 0xFFFF).tolist(), mb[real, 1].tolist(), sbm.tolist(),
+                        wb[t0:t1][real].tolist()))
+        assert ra == rb
         assert np.all(wb[t0:t1][~real] == 0)
         ca += qw_cost(ma)
         cb += qw_cost(mb)
+    assert cb < 0.85 * ca
+
+
+def test_brick_plan6_pair_lane_packing():
+    from pygrog_b200.calib._plan6 import BrickPlan6
+
+    rng = np.random.default_rng(19)
+    shape, kw = (24, 16, 40), 3
+    tgt, _, w = _toy_plan(shape, 6000, kw, rng, hot=3000)
+    idx = torch.from_numpy(rng.integers(0, 11 * 121, size=(6000, kw)).astype(np.int64))
+    a = BrickPlan6(tgt, idx, w, kw, shape, (4, 8, 8), n_outer=11, sub_cap=256, n_cta=3)
+    b = BrickPlan6(tgt, idx, w, kw, shape, (4, 8, 8), n_outer=11, sub_cap=256, n_cta=3, lane_order=True,
+                   pair_lanes=True, cell_order=True)
+
+    def cost(m):
+        """Quarter-warps of four replicas (two lanes each, half-row offset = 4
+        bank quads): largest number of distinct operators per class mod 4."""
+        tot = 0
+        for g0 in range(0, len(m), 4):
+            g = m[g0:g0 + 4]
+            g = g[g[:, 0] >= 0]
+            if len(g):
+                for ops in (np.unique(g[:, 1] & 0xFFFF), np.unique(g[:, 1] >> 16)):
+                    tot += np.bincount(ops % 4, minlength=4).max()
+        return tot
+
+    ca = cb = 0
+    for (r0, r1, _, _), (t0, t1, _, _) in zip(a.subs.numpy(), b.subs.numpy()):
+        ma = a.meta.numpy()[r0:r1].astype(np.int64)
+        mb = b.meta.numpy()[t0:t1].astype(np.int64)
+        real = mb[:, 0] >= 0
+        assert (t1 - t0) % 4 == 0 and t1 - t0 <= 256 and (t1 - t0) - (r1 - r0) < 4
+        assert sorted(zip((ma[:, 0] & 0xFFFF).tolist(), ma[:, 1].tolist())) == \
+            sorted(zip((mb[real, 0] & 0xFFFF).tolist(), mb[real, 1].tolist()))
+        ca += cost(ma)
+        cb += cost(mb)
     assert cb < 0.85 * ca
 
 
