@@ -309,6 +309,41 @@ def run_serving(dev, seconds: float, rate: float = 200.0, seed: int = 1004) -> d
     }
 
 
+def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
+    """Config c3: ``n_slices`` uneven 2-D radial slices (spokes U{13..233}, readout
+    U{256..768}, grid U{128..384}, coils U{8..32}), each GROG interpolation +
+    SparseFFT adjoint + 20 CG iterations, reconstructed as one batch of
+    independent requests (every slice its own resident protocol; the shapes
+    differ, so there is nothing to stack) on 4 streams, k-space from and images
+    to page-locked host memory.  Wall time of the batch, best of 3."""
+    import torch
+
+    from pygrog_b200.serve import ReconProtocol, ReconServer, Request
+    from pygrog_b200.workloads import c3_protocols
+
+    t0 = time.perf_counter()
+    protos = {}
+    for sp in c3_protocols(seed, n_slices):
+        kw = dict(sp)
+        name = kw.pop("name")
+        protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
+                                     device=dev, **kw)
+    server = ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=4, device=dev)
+    setup_s = time.perf_counter() - t0
+    gen = torch.Generator().manual_seed(seed)
+    data = {k: torch.randn(p.data_shape, dtype=torch.complex64, generator=gen).pin_memory() for k, p in protos.items()}
+    walls = []
+    for _ in range(4):  # first run warms the streams
+        reqs = [Request(i, k, 0.0, data[k]) for i, k in enumerate(protos)]
+        walls.append(server.run(reqs, realtime=False)["wall_s"])
+    wall = min(walls[1:])
+    sc = sum(p.C * int(np.prod(p.spatial)) for p in protos.values())
+    return {"slices": n_slices, "ms_per_batch": wall * 1e3, "sample_coils": sc,
+            "sample_coils_per_s": sc / wall, "recons_per_s": n_slices / wall, "cg_iters": 20,
+            "setup_s": setup_s,
+            "note": "wall time incl. host<->device copies; plans, tables, PSFs and CUDA graphs built in setup"}
+
+
 def cg_sense_c2(dev, iters: int = 30) -> dict:
     """Time per CG-SENSE iteration of config c2 (spiral 320^2, 16 coils, Toeplitz on 640^2),
     one CUDA graph of ``iters`` iterations, CUDA events."""
@@ -353,6 +388,7 @@ def main():
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="open-loop serving duration (0: skip)")
+    ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
     args = ap.parse_args()
     resized = (args.spokes, args.readout, args.grid) != (N_SPOKES, N_READOUT, GRID_N)
     N_SPOKES, N_READOUT, GRID_N = args.spokes, args.readout, args.grid
@@ -460,13 +496,18 @@ def main():
             "api": "GrogInterpolator.grid(pinned host tensor) + GrogInterpolator.degrid(host tensor)",
         }
 
-    serving = cg2 = None
+    serving = cg2 = c3 = None
     if ws == 1 and args.serve_seconds > 0 and not resized:
         try:
             cg2 = cg_sense_c2(dev)
             serving = run_serving(dev, args.serve_seconds)
         except Exception as exc:  # noqa: BLE001
             serving = {"error": f"{type(exc).__name__}: {exc}"}
+    if ws == 1 and args.c3_slices > 0 and not resized:
+        try:
+            c3 = c3_batch(dev, args.c3_slices)
+        except Exception as exc:  # noqa: BLE001
+            c3 = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank == 0:
         cpu = None
@@ -494,7 +535,7 @@ def main():
                              else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "kernels": list(bp.kernel_names()), "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode + ("/pairs" if getattr(bp, "pairs", False) else ""), "kernels": list(bp.kernel_names()), "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
             "fwd_ms": fwd_ms,
@@ -510,6 +551,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "cg_sense_c2": cg2,
+            "c3_batch": c3,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)

@@ -202,6 +202,14 @@ def serving_protocols(seed: int = 1004, n_slices: int = 2) -> list[dict]:
     w2 = config2()
     out.append(dict(name="c2", shape=w2.shape, coords=w2.coords, acr=w2.acr, smaps=w2.smaps, oversamp=2.0,
                     kernel_width=2, kernel_shape="circle", precision=1, lamda=1e-3, max_iter=30))
+    return out + c3_protocols(seed, n_slices)
+
+
+def c3_protocols(seed: int = 1004, n_slices: int = 64) -> list[dict]:
+    """The first ``n_slices`` uneven radial slices of c3 as ``ReconProtocol``
+    keyword sets (coil maps from seeded Gaussian bumps, ACR = centre 24^2 of the
+    coil k-space of a seeded phantom, 20 CG iterations)."""
+    out = []
     rng = np.random.default_rng(seed)
     for i, s in enumerate(config3_slices(seed=1003, n_slices=n_slices)):
         n, C = s["grid"], s["coils"]
