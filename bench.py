@@ -383,7 +383,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--table-mode", default=None, choices=["v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"])
+    ap.add_argument("--table-mode", default=None, choices=["tc", "tc1", "v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"])
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)

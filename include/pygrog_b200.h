@@ -335,6 +335,30 @@ PGB_API int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N
                                const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);
 
+/* Tensor-core (mma.sync bf16, fp32 accumulate) gridding: the same operator as
+ * the table path of calib/_grog.py:1283-1295 + operator/_sparse_fft.py:416
+ * (forward) and its adjoint, with the table applied in its exact eigen-factored
+ * form T = V2 D2[k] V2^-1 V1 D1[j] V1^-1 V0 D0[i] V0^-1 (calib/_grappa.py:62-72,
+ * 130-208: every per-axis operator is expm(d logm G)).  wfrag: int32
+ * (ndim + 1, 2, NFR, 32) bf16x2 head / tail B-fragment words of the dense
+ * stages in application order (calib/_tc.py), NFR = (CP/4) * (CP/4 rounded
+ * down to even + (CP/4) % 2), CP = C rounded up to a multiple of 4; dtab:
+ * complex64 (ndim, nsteps, CP) diagonal phases in application order.  terms: 3
+ * = bf16x3 split products (~1e-5 relative), 1 = plain bf16.  Plans: v6 plans
+ * built with n_outer = nsteps (meta.y = (e / nsteps) | (e % nsteps) << 16),
+ * sub_cap <= 256; C <= 16.  The plan's n_cta should be 148 x
+ * pgb_grog_tc_blocks_per_sm(C, ndim).  Same zeroing / primary / secondary /
+ * zero_src contract as pgb_grog_grid_v6 / pgb_grog_degrid_v6. */
+PGB_API size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t ndim, int64_t sub_cap);
+PGB_API int pgb_grog_tc_blocks_per_sm(int64_t C, int64_t ndim);
+PGB_API int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const void* wfrag,
+                             const void* dtab, int64_t nsteps, int64_t ndim, int64_t C, int64_t B, int64_t terms,
+                             const pgb_v6_plan* plan, void* stream);
+PGB_API int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N, const void* wfrag_h,
+                               const void* dtab_h, int64_t nsteps, int64_t ndim, int64_t C, int64_t B,
+                               int64_t terms, const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
+                               const int32_t* zero_src, int64_t n_zero, void* stream);
+
 /* Replica expansion of interpolate() (calib/_grog.py:668-695):
  * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]
  * data (B,C,N), out (B,C,N*kw); entries outside [0,K) give 0. C <= 32. */

@@ -137,6 +137,9 @@ _SIGS = {
     "pgb_dot_f64_noalloc": [_vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_grog_grid_v6": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
     "pgb_grog_degrid_v6": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
+    "pgb_grog_grid_tc": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp],
+    "pgb_grog_degrid_tc": [_vp, _i64, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
+    "pgb_grog_tc_blocks_per_sm": [_i64, _i64],
 }
 _SIZE_FUNCS = {
     "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],
@@ -144,6 +147,7 @@ _SIZE_FUNCS = {
     "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
     "pgb_grog_v6_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_grog_v8_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
+    "pgb_grog_tc_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_reduce_scratch_bytes": [],
 }
 

@@ -170,3 +170,34 @@ def KernelTable(
         outer, inner = table_factors(Gx, Gy, Gz, ndim)
         return table.numpy(), nsteps, ndim, (outer.to(out_dtype), inner.to(out_dtype))
     return table.numpy(), nsteps, ndim
+
+
+def eigen_factors(train_data, radius: float, precision: int = 1, lamda: float = 0.01,
+                  fit_dtype: torch.dtype | None = None) -> SimpleNamespace:
+    """Eigendecompositions of the per-axis shift generators behind the table.
+
+    The reference forms each fractional operator as ``G_a(d) = expm(d L_a)``
+    with ``L_a = logm(G_a)`` cast to the ACR's dtype (``_grappa.py:62-72,
+    184-208``).  With ``L_a = V_a diag(l_a) V_a^-1`` (complex128 ``eig``) this is
+    ``G_a(d) = V_a diag(exp(d l_a)) V_a^-1``, so the table product
+    ``T[i, j, k] = Gx(d_k) Gy(d_j) Gz(d_i)`` becomes fixed dense basis changes
+    with per-replica diagonal phases in between (the tensor-core gridder).
+
+    Returns ``ndim``, ``nsteps``, the float32 ``deltas`` and ``axes``: the
+    ``(V, l)`` pairs (complex128) in the order the forward applies them
+    (3-D: z, y, x; 2-D: y, x), matching the table index split
+    ``e = q * nsteps + k`` with ``q = i * nsteps + j`` (3-D) or ``q = i`` (2-D).
+    """
+    t = torch.as_tensor(np.asarray(train_data)) if isinstance(train_data, np.ndarray) else torch.as_tensor(train_data)
+    t = t.detach().cpu()
+    if fit_dtype is not None:
+        t = t.to(fit_dtype)
+    ops = train_grappa(t, lamda)
+    _, nsteps, deltas = shift_steps(radius, precision)
+    order = [ops.z, ops.y, ops.x] if ops.z is not None else [ops.y, ops.x]
+    axes = []
+    for G in order:
+        L = _logm(torch.as_tensor(G))
+        lam, V = torch.linalg.eig(L.to(torch.complex128))
+        axes.append((V, lam))
+    return SimpleNamespace(ndim=len(order), nsteps=int(nsteps), deltas=deltas, axes=axes)

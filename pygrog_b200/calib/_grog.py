@@ -34,7 +34,7 @@ import torch
 
 from .. import _lib
 from ._grappa import KernelTable
-from ._plan6 import BrickPlan6, lane_chunk
+from ._plan6 import BrickPlan6, _sm_count, lane_chunk
 
 _DEFAULT_DEVICE = "cuda"
 
@@ -479,7 +479,7 @@ class GrogGridder:
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
 
     def __init__(self, target_idx, interp_idx, rep_weight, kw, grid_shape, table, factors, nsteps,
-                 mode: str | None = None, brick=None, chunk: int = 2048):
+                 mode: str | None = None, brick=None, chunk: int = 2048, tc_ops: dict | None = None):
         C = int(table.shape[-1])
         K = int(table.shape[0])
         self.C = C
@@ -488,6 +488,10 @@ class GrogGridder:
         cand = self.BRICKS3 if ndim == 3 else self.BRICKS2
         if brick is not None:
             cand = (tuple(brick),)
+        self.tc = None
+        if mode in ("tc", "tc1"):
+            self._init_tc(mode, tc_ops, target_idx, interp_idx, rep_weight, kw, grid_shape, cand, lib)
+            return
         n_fact = int(factors[1].shape[0]) if factors is not None else None
 
         def v3_fits(n_inner, br):
@@ -639,6 +643,44 @@ class GrogGridder:
             if self.plan.n_valid > self.adj_plan.n_valid:
                 self.plan2 = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kwargs)
 
+    def _init_tc(self, mode, tc_ops, target_idx, interp_idx, rep_weight, kw, grid_shape, cand, lib):
+        """Tensor-core gridder (``csrc/grog_tc.cu``): sample-ordered v6 plans
+        with ``n_outer = nsteps`` and the eigen-factored table operands."""
+        C = self.C
+        if tc_ops is None:
+            raise ValueError("tensor-core gridding needs the eigen-factored table (calc_interp_table first)")
+        if C > 16:
+            raise ValueError("tc kernels cover C <= 16")
+        nd, nsteps = int(tc_ops["ndim"]), int(tc_ops["nsteps"])
+        if nd != len(grid_shape):
+            raise ValueError("table and plan dimensionality differ")
+        bps = int(lib.pgb_grog_tc_blocks_per_sm(C, nd))
+        budget = _SMEM_V3 if bps <= 1 else (_SMEM_V3 // bps) - 1024
+        chosen = None
+        for br in cand:
+            cells = br[0] * br[1] * br[2]
+            if lib.pgb_grog_tc_smem_bytes(C, cells, nsteps, nd, 256) <= budget:
+                chosen = tuple(br)
+                break
+        if chosen is None:
+            raise ValueError("tc kernels: no brick fits shared memory")
+        self.mode = mode
+        self.brick = chosen
+        self.sub_cap = 256
+        self.tc = tc_ops
+        self.terms = 3 if mode == "tc" else 1
+        self.n_outer = nsteps
+        self.fwd6 = None
+        self.pairs = False
+        dev = target_idx.device
+        kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True)
+        self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, **kwt)
+        first = _first_valid_mask(target_idx, kw)
+        self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwt)
+        self.plan2 = None
+        if self.plan.n_valid > self.adj_plan.n_valid:
+            self.plan2 = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kwt)
+
     @property
     def n_valid(self):
         return self.plan.n_valid
@@ -646,6 +688,8 @@ class GrogGridder:
     def kernel_names(self) -> tuple[str, str]:
         """Names of the (forward, adjoint) main kernels of this gridder."""
         m = self.mode
+        if m in ("tc", "tc1"):
+            return "grog_grid_tc_kernel", "grog_degrid_tc_kernel"
         if m == "v8":
             return ("grog_grid_v6_kernel" if self.fwd6 is not None else "grog_grid_v8_kernel", "grog_degrid_v8_kernel")
         k = {"v6": "v6_kernel", "v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(m, "factored_kernel")
@@ -654,10 +698,10 @@ class GrogGridder:
     def launches_per_call(self, adjoint: bool) -> int:
         bp = self.plan
         if adjoint:
-            if self.mode in ("v3", "v5", "v6", "v8"):
+            if self.mode in ("v3", "v5", "v6", "v8", "tc", "tc1"):
                 return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
             return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
-        if self.mode in ("v6", "v8"):
+        if self.mode in ("v6", "v8", "tc", "tc1"):
             return 1 + (1 if bp.zero_bricks.numel() else 0)
         return 1 + (1 if bp.split_bricks.numel() else 0)
 
@@ -671,7 +715,11 @@ class GrogGridder:
         G = out.shape[-1]
         bp = self.plan
         st = _lib.stream_ptr(data.device)
-        if self.mode == "v8" and self.fwd6 is not None:
+        if self.tc is not None:
+            wf, dt = self.tc["fwd"]
+            _lib.call("pgb_grog_grid_tc", data.data_ptr(), N, out.data_ptr(), G, wf.data_ptr(), dt.data_ptr(),
+                      self.tc["nsteps"], self.tc["ndim"], C, B, self.terms, _ctypes_ref(bp._c), st)
+        elif self.mode == "v8" and self.fwd6 is not None:
             olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
             _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
                       self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
@@ -699,7 +747,13 @@ class GrogGridder:
         bp = self.adj_plan
         st = _lib.stream_ptr(grid.device)
         zs = bp.zero_src.data_ptr() if bp.zero_src.numel() else None
-        if self.mode == "v8":
+        if self.tc is not None:
+            wf, dt = self.tc["adj"]
+            sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
+            _lib.call("pgb_grog_degrid_tc", grid.data_ptr(), G, out.data_ptr(), N, wf.data_ptr(), dt.data_ptr(),
+                      self.tc["nsteps"], self.tc["ndim"], C, B, self.terms, _ctypes_ref(bp._c), sec, zs,
+                      int(bp.zero_src.numel()), st)
+        elif self.mode == "v8":
             sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
             _lib.call("pgb_grog_degrid_v9" if self.pairs else "pgb_grog_degrid_v8", grid.data_ptr(), G,
                       out.data_ptr(), N, self.inner_h.data_ptr(),
@@ -821,6 +875,19 @@ class GrogInterpolator:
         self._interp_idx = idx
         self._interpolator_set = True
         self._brick_plans = None
+        self._fit_args = (train_data, float(self.plan.radius), precision, lamda, fit_dtype)
+        self._tc_ops = None
+
+    def _tc_operands(self) -> dict:
+        """Eigen-factored table operands of the tensor-core gridder (built once)."""
+        if getattr(self, "_tc_ops", None) is None:
+            from ._grappa import eigen_factors
+            from ._tc import tc_operands
+
+            train, radius, precision, lamda, fit_dtype = self._fit_args
+            ef = eigen_factors(train, radius, precision, lamda, fit_dtype)
+            self._tc_ops = tc_operands(ef, int(self._interp_kernel.shape[-1]), self.device)
+        return self._tc_ops
 
     def set_dataset_shape(self, shape):
         if self._dataset_shape_set:
@@ -889,8 +956,10 @@ class GrogInterpolator:
             sw = torch.sqrt(w)
             rep_w = sw * sw
             idx = self._interp_idx.reshape(s_total, -1)[s]
+            mode = getattr(self, "gridder_mode", None)
+            tc_ops = self._tc_operands() if mode in ("tc", "tc1") else None
             bp = GrogGridder(tgt, idx, rep_w, kw, plan.grid_shape, self._interp_kernel, self._factors,
-                             self._nsteps, mode=getattr(self, "gridder_mode", None))
+                             self._nsteps, mode=mode, tc_ops=tc_ops)
             self._brick_plans[s] = bp
         return bp
 

@@ -73,6 +73,7 @@ class BrickPlan6:
         cell_order: bool = False,
         seg_len: int = 8,
         pair_lanes: bool = False,
+        sample_order: bool = False,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -176,6 +177,12 @@ class BrickPlan6:
             src = spread(src, -1)
             cl = spread(cl, cells)  # padding: no cell
             sub_id = sub_full
+        elif sample_order:
+            # keep step (1)'s sample order: the tensor-core gridder reads each
+            # m-tile's staged samples in order (conflict-free) and spreads
+            # the cells of a tile
+            self.meta = torch.stack([cl | (slot << 16), q | (k << 16)], dim=1).to(torch.int32).contiguous()
+            self.w = w.contiguous()
         else:
             key2 = ((sub_id * self.n_outer + k) * n_in + q) * cells + cl
             _, p2 = torch.sort(key2, stable=True)

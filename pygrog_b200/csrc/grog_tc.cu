@@ -1,0 +1,791 @@
+// grog_tc.cu -- fused GROG grid / degrid on the tensor cores (bf16x3 or bf16).
+//
+// The table factorises exactly.  The reference builds every per-axis
+// fractional operator as G_a(d) = expm(d * L_a) with L_a = logm(G_a)
+// (calib/_grappa.py:62-72, 184-208) and the table as the product
+// T[i, j, k] = Gx(d_k) Gy(d_j) Gz(d_i) (calib/_grappa.py:130-181).  With the
+// eigendecomposition L_a = V_a diag(l_a) V_a^-1 that is
+//
+//   T x = Vx Dx[k] Vx^-1 Vy Dy[j] Vy^-1 Vz Dz[i] Vz^-1 x,   D_a[s] = diag(exp(d_s l_a)),
+//
+// i.e. four dense C x C matrices W0 = Vz^-1, W1 = Vy^-1 Vz, W2 = Vx^-1 Vy,
+// W3 = Vx shared by every replica, and three per-replica diagonals (two
+// dense stages fewer in 2-D).  The dense stages are GEMMs over all replicas
+// with no binning: each warp takes 16 replicas as the M rows of
+// mma.m16n8k16 / m16n8k8 (bf16 in, fp32 accumulate), the complex C x C
+// matrix realified with (re, im) interleaved so that an accumulator
+// fragment of one stage is, register for register, the A fragment of the
+// next, and the diagonal phases are lane-local complex products between
+// stages.  The W fragments live in registers for the whole kernel; the
+// diagonal tables (nsteps x C per axis) in shared memory.
+//
+// Precision: with terms == 3 every operand is split into a bf16 head and a
+// bf16 tail (x = hi + lo) and each product is hi*hi + hi*lo + lo*hi with fp32
+// accumulation (~2^-16 relative per stage); terms == 1 uses the heads only.
+//
+// Plans: the v6 brick plans (calib/_plan6.py) with n_outer = nsteps, i.e.
+// meta.y = q | k << 16 with q = e / nsteps and k = e % nsteps; in 3-D the
+// axis indices are (i, j, k) = (q / nsteps, q % nsteps, k), in 2-D (q, k).
+// Any replica order inside a sub-chunk is correct (sample order keeps the
+// staged-sample reads conflict-free).
+//
+//   forward:  per sub-chunk, stage the samples' coils (cp.async, double
+//             buffered), run the chain for 16 replicas per warp, add w * y to
+//             the brick tile with shared atomics; flush the tile once per
+//             brick (global atomics only for bricks split over CTAs)
+//   adjoint:  tile of the brick (cp.async, prefetched one brick ahead), the
+//             adjoint chain W3^H conj(Dx) W2^H conj(Dy) W1^H conj(Dz) W0^H per
+//             replica, w * y into a per-slot result buffer, flushed per
+//             sub-chunk (atomic adds for the secondary replicas)
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace pgb {
+namespace tc {
+
+constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk
+constexpr int kLast = 2, kSplit = 4;
+
+template <int CP>
+struct Shape {
+  static constexpr int NT = CP / 4;                   // n-tiles of 8 real columns (4 complex coils)
+  static constexpr int K16 = NT / 2;                  // k16 chunks of the next stage
+  static constexpr int K8 = NT % 2;                   // trailing k8 chunk
+  static constexpr int NFR = NT * (2 * K16 + K8);     // B-fragment words per lane per matrix
+  static constexpr int TS = CP + 1;                   // tile stride per cell (float2): conflict-free flush
+};
+
+template <int CP, int NS>
+struct Regs {
+  static constexpr int W = (NS + 1) * 2 * Shape<CP>::NFR;
+  static constexpr int MINB = W <= 80 ? 2 : 1;  // CTAs per SM the register budget allows
+};
+
+struct Geom {
+  int gz, gy, gx;
+  int bz, by, bx;
+  int lbx, lby;
+  int nbz, nby, nbx;
+};
+
+__device__ __forceinline__ void origin(const Geom& g, int brick, int& z0, int& y0, int& x0) {
+  const int bxy = g.nby * g.nbx;
+  const int biz = brick / bxy;
+  const int rem = brick - biz * bxy;
+  const int biy = rem / g.nbx;
+  z0 = biz * g.bz;
+  y0 = biy * g.by;
+  x0 = (rem - biy * g.nbx) * g.bx;
+}
+
+__device__ __forceinline__ bool flat_of(const Geom& g, int z0, int y0, int x0, int cl, int64_t& flat) {
+  const int x = x0 + (cl & (g.bx - 1));
+  const int y = y0 + ((cl >> g.lbx) & (g.by - 1));
+  const int z = z0 + (cl >> (g.lbx + g.lby));
+  if (z >= g.gz || y >= g.gy || x >= g.gx) return false;
+  flat = (static_cast<int64_t>(z) * g.gy + y) * g.gx + x;
+  return true;
+}
+
+__device__ __forceinline__ void cp8(void* smem_dst, const void* gsrc, int bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void wait_groups() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// d += A B, A 16x16 (4 bf16x2 words), B 16x8 (2 words), fp32 accumulate
+__device__ __forceinline__ void mma16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                      uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// d += A B, A 16x8 (2 words), B 8x8 (1 word)
+__device__ __forceinline__ void mma8(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+// (re, im) -> bf16x2 head (re in the low half) and tail
+__device__ __forceinline__ void split2(float2 v, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+  const float2 hf = __bfloat1622float2(h);
+  hi = bf2_bits(h);
+  lo = bf2_bits(__floats2bfloat162_rn(v.x - hf.x, v.y - hf.y));
+}
+
+// v[r][m] = complex coil 4 m + t of row g + 8 r of the lane's m-tile (g = lane / 4,
+// t = lane % 4).  One dense stage: v <- v W^T over the 16 rows, W's fragments
+// bh (heads) / bl (tails).
+template <int CP, int TERMS>
+__device__ __forceinline__ void mm_stage(float2 (&v)[2][Shape<CP>::NT], const uint32_t (&bh)[Shape<CP>::NFR],
+                                         const uint32_t (&bl)[Shape<CP>::NFR]) {
+  constexpr int NT = Shape<CP>::NT, K16 = Shape<CP>::K16, K8 = Shape<CP>::K8;
+  uint32_t ah[2][NT], al[2][NT];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+#pragma unroll
+    for (int m = 0; m < NT; ++m) {
+      if constexpr (TERMS == 3) {
+        split2(v[r][m], ah[r][m], al[r][m]);
+      } else {
+        ah[r][m] = bf2_bits(__floats2bfloat162_rn(v[r][m].x, v[r][m].y));
+        al[r][m] = 0u;
+      }
+    }
+  }
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    int f = nt * (2 * K16 + K8);
+#pragma unroll
+    for (int kc = 0; kc < K16; ++kc) {
+      if constexpr (TERMS == 3) {
+        mma16(d, al[0][2 * kc], al[1][2 * kc], al[0][2 * kc + 1], al[1][2 * kc + 1], bh[f], bh[f + 1]);
+        mma16(d, ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bl[f], bl[f + 1]);
+      }
+      mma16(d, ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bh[f], bh[f + 1]);
+      f += 2;
+    }
+    if constexpr (K8) {
+      if constexpr (TERMS == 3) {
+        mma8(d, al[0][NT - 1], al[1][NT - 1], bh[f]);
+        mma8(d, ah[0][NT - 1], ah[1][NT - 1], bl[f]);
+      }
+      mma8(d, ah[0][NT - 1], ah[1][NT - 1], bh[f]);
+    }
+    v[0][nt] = make_float2(d[0], d[1]);
+    v[1][nt] = make_float2(d[2], d[3]);
+  }
+}
+
+// W fragments of all NS + 1 stages, global layout (stage, head/tail, word, lane)
+template <int CP, int NS>
+__device__ __forceinline__ void load_w(const uint32_t* __restrict__ wfrag, int lane,
+                                       uint32_t (&wb)[NS + 1][2][Shape<CP>::NFR]) {
+  constexpr int NFR = Shape<CP>::NFR;
+#pragma unroll
+  for (int s = 0; s <= NS; ++s)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int f = 0; f < NFR; ++f) wb[s][b][f] = __ldg(wfrag + ((s * 2 + b) * NFR + f) * 32 + lane);
+}
+
+// One replica row's decoded metadata.
+struct Row {
+  int cell, slot, ix0, ix1, ix2;
+  float w;
+  bool on;
+};
+
+template <int NS>
+__device__ __forceinline__ Row decode(int2 m, float w, bool in_range, int cells, int nu, int nsteps) {
+  Row r;
+  r.cell = m.x & 0xFFFF;
+  r.slot = static_cast<int>(static_cast<unsigned>(m.x) >> 16);
+  const int q = m.y & 0xFFFF;
+  const int k = static_cast<int>(static_cast<unsigned>(m.y) >> 16);
+  const int nq = NS == 3 ? nsteps * nsteps : nsteps;
+  r.on = in_range && m.x >= 0 && r.cell < cells && r.slot < nu && q < nq && k < nsteps;
+  if (!r.on) {
+    r.cell = 0;
+    r.slot = 0;
+    r.ix0 = r.ix1 = r.ix2 = 0;
+    r.w = 0.f;
+    return r;
+  }
+  if constexpr (NS == 3) {
+    r.ix0 = q / nsteps;
+    r.ix1 = q - r.ix0 * nsteps;
+    r.ix2 = k;
+  } else {
+    r.ix0 = q;
+    r.ix1 = k;
+    r.ix2 = 0;
+  }
+  r.w = w;
+  return r;
+}
+
+template <int NS, bool ADJ>
+__device__ __forceinline__ int diag_index(const Row& r, int s) {
+  const int a = ADJ ? NS - 1 - s : s;
+  return a == 0 ? r.ix0 : (a == 1 ? r.ix1 : r.ix2);
+}
+
+// The whole chain on one m-tile: NS + 1 dense stages with the diagonal phases
+// of table dt (NS, nsteps, CP) between them.
+template <int CP, int NS, int TERMS, bool ADJ>
+__device__ __forceinline__ void chain(float2 (&v)[2][Shape<CP>::NT], const uint32_t (&wb)[NS + 1][2][Shape<CP>::NFR],
+                                      const float2* __restrict__ dt, int nsteps, const Row (&rw)[2], int t) {
+  constexpr int NT = Shape<CP>::NT;
+#pragma unroll
+  for (int s = 0; s <= NS; ++s) {
+    mm_stage<CP, TERMS>(v, wb[s][0], wb[s][1]);
+    if (s < NS) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[r], s)) * CP + t;
+#pragma unroll
+        for (int m = 0; m < NT; ++m) v[r][m] = cmul(v[r][m], drow[4 * m]);
+      }
+    }
+  }
+}
+
+// Minimal per-CTA stream of sub-chunk descriptors, two ahead.
+struct Stream {
+  const int4* sd;
+  const int2* si;
+  int p, p1;
+  int4 d0, d1, d2;
+  int2 i0, i1;
+  __device__ __forceinline__ int4 ld_d(int q) const { return q < p1 ? __ldg(sd + q) : make_int4(0, 0, 0, 0); }
+  __device__ __forceinline__ int2 ld_i(int q) const { return q < p1 ? __ldg(si + q) : make_int2(0, 0); }
+  __device__ __forceinline__ void init(const int4* sd_, const int2* si_, int p0_, int p1_) {
+    sd = sd_;
+    si = si_;
+    p = p0_;
+    p1 = p1_;
+    d0 = ld_d(p);
+    d1 = ld_d(p + 1);
+    d2 = ld_d(p + 2);
+    i0 = ld_i(p);
+    i1 = ld_i(p + 1);
+  }
+  __device__ __forceinline__ void advance() {
+    ++p;
+    d0 = d1;
+    d1 = d2;
+    i0 = i1;
+    d2 = ld_d(p + 2);
+    i1 = ld_i(p + 1);
+  }
+};
+
+__device__ __forceinline__ int n_slots(int4 d, int cap) { return min(max(d.w - d.z, 0), cap); }
+__device__ __forceinline__ int n_reps(int4 d, int cap) { return min(max(d.y - d.x, 0), cap); }
+
+// Metadata of this lane's four rows (two m-tiles x rows g, g + 8) of sub-chunk d.
+struct LaneMeta {
+  int2 m[2][2];
+  float w[2][2];
+};
+__device__ __forceinline__ void load_meta(LaneMeta& lm, const int2* __restrict__ meta, const float* __restrict__ wts,
+                                          int4 d, bool valid, int cap, int warp, int g) {
+  const int nr = valid ? n_reps(d, cap) : 0;
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int row = (warp + 8 * j) * 16 + 8 * r + g;
+      if (row < nr) {
+        lm.m[j][r] = __ldg(meta + d.x + row);
+        lm.w[j][r] = __ldg(wts + d.x + row);
+      } else {
+        lm.m[j][r] = make_int2(-1, 0);
+        lm.w[j][r] = 0.f;
+      }
+    }
+}
+
+// Shared-memory layout in float2 units: diagonal tables | tile(s) | staging (x or results)
+struct Smem {
+  int dt, tile, tile_sz, xs, xs_sz, total;
+  __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward) {
+    dt = 0;
+    tile = (NS * nsteps * CP + 1) & ~1;
+    tile_sz = (cells * (CP + 1) + 1) & ~1;
+    xs = tile + (forward ? 1 : 2) * tile_sz;
+    xs_sz = CP * (cap + 4);
+    total = xs + (forward ? 2 : 1) * xs_sz;
+  }
+};
+
+template <int CP, int NS, int TERMS>
+__global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
+    const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G, int C,
+    const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
+    const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
+    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
+  extern __shared__ float4 smem4[];
+  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, TS = Shape<CP>::TS;
+  const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
+  if (p0 >= p1) return;  // block-uniform
+  const int cells = geom.bz * geom.by * geom.bx;
+  const Smem lay(CP, NS, nsteps, cells, cap, true);
+  const int XS = cap + 4;
+  float2* base = reinterpret_cast<float2*>(smem4);
+  float2* dt = base + lay.dt;
+  float2* tile = base + lay.tile;
+  float2* xs0 = base + lay.xs;
+  const int b = blockIdx.y;
+  const float2* dat = data + static_cast<int64_t>(b) * C * N;
+  float2* grd = grid + static_cast<int64_t>(b) * C * G;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+
+  auto stage_x = [&](int4 d, float2* xs) {  // samples' coils of sub-chunk d, coil-major
+    const int nu = n_slots(d, cap);
+    if (tid < nu) {
+      const int u = __ldg(uniq + d.z + tid);
+      const bool ok = u >= 0 && u < N;
+      for (int c = 0; c < C; ++c)
+        cp8(xs + c * XS + tid, ok ? dat + static_cast<int64_t>(c) * N + u : dat, ok ? 8 : 0);
+    }
+  };
+
+  Stream st;
+  st.init(sd, si, p0, p1);
+  stage_x(st.d0, xs0);
+  commit();
+  uint32_t wb[NS + 1][2][NFR];
+  load_w<CP, NS>(wfrag, lane, wb);
+  for (int i = tid; i < NS * nsteps * CP; i += kT) dt[i] = __ldg(dtab + i);
+  for (int i = tid; i < lay.tile_sz; i += kT) tile[i] = make_float2(0.f, 0.f);
+  LaneMeta lm, ln;
+  load_meta(lm, meta, wts, st.d0, true, cap, warp, g);
+
+  int buf = 0;
+  while (true) {
+    const bool more = st.p + 1 < p1;
+    if (more) {
+      stage_x(st.d1, xs0 + (buf ^ 1) * lay.xs_sz);
+      commit();
+      wait_groups<1>();
+    } else {
+      wait_groups<0>();
+    }
+    load_meta(ln, meta, wts, st.d1, more, cap, warp, g);
+    __syncthreads();  // staging buffer `buf` complete; tile zeroed / flushed
+    {
+      const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
+      const float2* xs = xs0 + buf * lay.xs_sz;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int mt = warp + 8 * j;
+        if (mt * 16 >= nr) break;  // warp-uniform
+        Row rw[2];
+        float2 v[2][NT];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          rw[r] = decode<NS>(lm.m[j][r], lm.w[j][r], mt * 16 + 8 * r + g < nr, cells, nu, nsteps);
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            const int c = 4 * m + t;
+            v[r][m] = (rw[r].on && c < C) ? xs[c * XS + rw[r].slot] : make_float2(0.f, 0.f);
+          }
+        }
+        chain<CP, NS, TERMS, false>(v, wb, dt, nsteps, rw, t);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          if (!rw[r].on) continue;
+          float2* dst = tile + rw[r].cell * TS;
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            const int c = 4 * m + t;
+            if (c < C) {
+              atomicAdd(&dst[c].x, rw[r].w * v[r][m].x);
+              atomicAdd(&dst[c].y, rw[r].w * v[r][m].y);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // tile complete for this sub-chunk; staging buffer `buf` free
+    if (st.i0.y & kLast) {
+      int z0, y0, x0;
+      origin(geom, st.i0.x, z0, y0, x0);
+      const bool split = (st.i0.y & kSplit) != 0;
+      for (int i = tid; i < C * cells; i += kT) {
+        const int c = i / cells;
+        const int cl = i - c * cells;
+        const float2 v = tile[cl * TS + c];
+        tile[cl * TS + c] = make_float2(0.f, 0.f);  // this thread re-zeroes what it flushed
+        int64_t flat;
+        if (!flat_of(geom, z0, y0, x0, cl, flat)) continue;
+        float2* dst = grd + static_cast<int64_t>(c) * G + flat;
+        if (split) {
+          if (v.x != 0.f || v.y != 0.f) {
+            atomicAdd(&dst->x, v.x);
+            atomicAdd(&dst->y, v.y);
+          }
+        } else {
+          *dst = v;
+        }
+      }
+    }
+    if (!more) break;
+    st.advance();
+    lm = ln;
+    buf ^= 1;
+  }
+}
+
+template <int CP, int NS, int TERMS, bool ACC>
+__global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
+    const float2* __restrict__ grid, int64_t G, float2* __restrict__ out, int64_t N, int C,
+    const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
+    const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
+    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
+  extern __shared__ float4 smem4[];
+  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, TS = Shape<CP>::TS;
+  const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
+  if (p0 >= p1) return;
+  const int cells = geom.bz * geom.by * geom.bx;
+  const Smem lay(CP, NS, nsteps, cells, cap, false);
+  const int XS = cap + 4;
+  float2* base = reinterpret_cast<float2*>(smem4);
+  float2* dt = base + lay.dt;
+  float2* tiles = base + lay.tile;  // 2 x (cells, TS)
+  float2* res = base + lay.xs;      // (CP, XS) per-slot results
+  const int b = blockIdx.y;
+  const float2* grd = grid + static_cast<int64_t>(b) * C * G;
+  float2* o = out + static_cast<int64_t>(b) * C * N;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+
+  auto issue_tile = [&](int brick, float2* tl) {
+    int z0, y0, x0;
+    origin(geom, brick, z0, y0, x0);
+    for (int i = tid; i < C * cells; i += kT) {
+      const int c = i / cells;
+      const int cl = i - c * cells;
+      int64_t flat;
+      const bool in = flat_of(geom, z0, y0, x0, cl, flat);
+      cp8(tl + cl * TS + c, in ? grd + static_cast<int64_t>(c) * G + flat : grd, in ? 8 : 0);
+    }
+  };
+  auto ld_u = [&](int4 d, bool valid) -> int {
+    return (valid && tid < n_slots(d, cap)) ? __ldg(uniq + d.z + tid) : -1;
+  };
+
+  Stream st;
+  st.init(sd, si, p0, p1);
+  int par = 0;
+  issue_tile(st.i0.x, tiles);
+  commit();
+  uint32_t wb[NS + 1][2][NFR];
+  load_w<CP, NS>(wfrag, lane, wb);
+  for (int i = tid; i < NS * nsteps * CP; i += kT) dt[i] = __ldg(dtab + i);
+  for (int i = tid; i < lay.xs_sz; i += kT) res[i] = make_float2(0.f, 0.f);
+  LaneMeta lm, ln;
+  load_meta(lm, meta, wts, st.d0, true, cap, warp, g);
+  int u0 = ld_u(st.d0, true);
+
+  while (true) {
+    const bool more = st.p + 1 < p1;
+    const bool last = (st.i0.y & kLast) != 0;
+    if (last && more) {  // next brick's tile into the other buffer during this compute
+      issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz);
+      commit();
+      wait_groups<1>();
+    } else {
+      wait_groups<0>();
+    }
+    load_meta(ln, meta, wts, st.d1, more, cap, warp, g);
+    const int u1 = ld_u(st.d1, more);
+    __syncthreads();  // tile of this brick complete; previous results flushed
+    {
+      const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
+      const float2* tl = tiles + par * lay.tile_sz;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int mt = warp + 8 * j;
+        if (mt * 16 >= nr) break;  // warp-uniform
+        Row rw[2];
+        float2 v[2][NT];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          rw[r] = decode<NS>(lm.m[j][r], lm.w[j][r], mt * 16 + 8 * r + g < nr, cells, nu, nsteps);
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            const int c = 4 * m + t;
+            v[r][m] = (rw[r].on && c < C) ? tl[rw[r].cell * TS + c] : make_float2(0.f, 0.f);
+          }
+        }
+        chain<CP, NS, TERMS, true>(v, wb, dt, nsteps, rw, t);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          if (!rw[r].on) continue;
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            const int c = 4 * m + t;
+            if (c < C) {
+              float2* dst = res + c * XS + rw[r].slot;
+              if (ACC) {
+                atomicAdd(&dst->x, rw[r].w * v[r][m].x);
+                atomicAdd(&dst->y, rw[r].w * v[r][m].y);
+              } else {
+                *dst = make_float2(rw[r].w * v[r][m].x, rw[r].w * v[r][m].y);
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // results complete; this brick's tile no longer read
+    if (tid < n_slots(st.d0, cap)) {
+      const bool ok = u0 >= 0 && u0 < N;
+      for (int c = 0; c < C; ++c) {
+        float2* rv = res + c * XS + tid;
+        const float2 v = *rv;
+        if (ACC) *rv = make_float2(0.f, 0.f);  // this thread re-clears what it flushed
+        if (!ok) continue;
+        float2* dst = o + static_cast<int64_t>(c) * N + u0;
+        if (ACC) {
+          atomicAdd(&dst->x, v.x);
+          atomicAdd(&dst->y, v.y);
+        } else {
+          *dst = v;
+        }
+      }
+    }
+    if (!more) break;
+    if (last) par ^= 1;
+    st.advance();
+    lm = ln;
+    u0 = u1;
+  }
+}
+
+__global__ void zero_bricks_tc(float2* __restrict__ grid, int64_t G, int C, int B,
+                               const int32_t* __restrict__ bricks, int n_bricks, Geom geom) {
+  const int cells = geom.bz * geom.by * geom.bx;
+  const int64_t total = static_cast<int64_t>(n_bricks) * cells;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int bi = static_cast<int>(i / cells);
+    const int cl = static_cast<int>(i - static_cast<int64_t>(bi) * cells);
+    int z0, y0, x0;
+    origin(geom, bricks[bi], z0, y0, x0);
+    int64_t flat;
+    if (!flat_of(geom, z0, y0, x0, cl, flat)) continue;
+    for (int b = 0; b < B; ++b)
+      for (int c = 0; c < C; ++c) grid[(static_cast<int64_t>(b) * C + c) * G + flat] = make_float2(0.f, 0.f);
+  }
+}
+
+__global__ void zero_samples_tc(float2* __restrict__ out, int64_t N, int C, int B, const int32_t* __restrict__ src,
+                                int64_t n) {
+  const int64_t total = n * C * B;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = i % n;
+    const int64_t bc = i / n;
+    const int64_t s = src[k];
+    if (s >= 0 && s < N) out[bc * N + s] = make_float2(0.f, 0.f);
+  }
+}
+
+inline int padded(int64_t C) { return static_cast<int>((C + 3) / 4 * 4); }
+
+static int geom_of(const pgb_v6_plan* p, Geom& g, const char* who) {
+  PGB_REQUIRE(p != nullptr, PGB_ERR_INVALID, "%s: null plan", who);
+  auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
+  PGB_REQUIRE(pow2(p->bz) && pow2(p->by) && pow2(p->bx) && p->gz >= 1 && p->gy >= 1 && p->gx >= 1,
+              PGB_ERR_INVALID, "%s: brick extents must be powers of two", who);
+  const int64_t cells = static_cast<int64_t>(p->bz) * p->by * p->bx;
+  PGB_REQUIRE(cells <= 4096, PGB_ERR_RANGE, "%s: brick of %lld cells exceeds 4096", who, (long long)cells);
+  PGB_REQUIRE(p->nbz == (p->gz + p->bz - 1) / p->bz && p->nby == (p->gy + p->by - 1) / p->by &&
+                  p->nbx == (p->gx + p->bx - 1) / p->bx,
+              PGB_ERR_INVALID, "%s: brick counts do not match the grid", who);
+  PGB_REQUIRE(p->n_cta >= 0 && p->n_cta <= 65535 && p->sub_cap >= 1 && p->sub_cap <= kT, PGB_ERR_INVALID,
+              "%s: invalid CTA count or sub-chunk capacity (1..%d)", who, kT);
+  PGB_REQUIRE(p->n_cta == 0 || (p->cta_ptr && p->sd && p->si && p->uniq && p->meta && p->w), PGB_ERR_INVALID,
+              "%s: null plan arrays", who);
+  int lbx = 0, lby = 0;
+  while ((1 << lbx) < p->bx) ++lbx;
+  while ((1 << lby) < p->by) ++lby;
+  g = Geom{p->gz, p->gy, p->gx, p->bz, p->by, p->bx, lbx, lby, p->nbz, p->nby, p->nbx};
+  return PGB_OK;
+}
+
+static int check_common(const char* who, int64_t C, int64_t N, int64_t B, int64_t nsteps, int64_t ndim,
+                        int64_t terms, const void* wfrag, const void* dtab) {
+  PGB_REQUIRE(C >= 1 && C <= 16, PGB_ERR_UNSUPPORTED, "%s: ncoils must be 1..16, got %lld", who, (long long)C);
+  PGB_REQUIRE(ndim == 2 || ndim == 3, PGB_ERR_INVALID, "%s: ndim must be 2 or 3", who);
+  PGB_REQUIRE(terms == 1 || terms == 3, PGB_ERR_INVALID, "%s: terms must be 1 (bf16) or 3 (bf16x3)", who);
+  PGB_REQUIRE(nsteps >= 1 && nsteps <= (ndim == 3 ? 255 : 65535), PGB_ERR_RANGE, "%s: invalid nsteps %lld", who,
+              (long long)nsteps);
+  PGB_REQUIRE(N >= 0 && N < (int64_t(1) << 31) && B >= 0 && B <= 65535, PGB_ERR_RANGE, "%s: invalid N/B", who);
+  PGB_REQUIRE(wfrag != nullptr && dtab != nullptr, PGB_ERR_INVALID, "%s: null fragment or phase table", who);
+  return PGB_OK;
+}
+
+}  // namespace tc
+}  // namespace pgb
+
+using namespace pgb;
+using namespace pgb::tc;
+
+#define PGB_TC_DISPATCH(X) \
+  X(4, 2) X(4, 3) X(8, 2) X(8, 3) X(12, 2) X(12, 3) X(16, 2) X(16, 3)
+
+extern "C" {
+
+size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t ndim, int64_t sub_cap) {
+  if (C < 1 || C > 16 || cells < 1 || cells > 4096 || nsteps < 1 || nsteps > 65535 || (ndim != 2 && ndim != 3) ||
+      sub_cap < 1 || sub_cap > kT)
+    return ~static_cast<size_t>(0);
+  const int CP = padded(C), NS = static_cast<int>(ndim);
+  const size_t a = Smem(CP, NS, static_cast<int>(nsteps), static_cast<int>(cells), static_cast<int>(sub_cap), true).total;
+  const size_t b = Smem(CP, NS, static_cast<int>(nsteps), static_cast<int>(cells), static_cast<int>(sub_cap), false).total;
+  return (a > b ? a : b) * sizeof(float2);
+}
+
+int pgb_grog_tc_blocks_per_sm(int64_t C, int64_t ndim) {
+  if (C < 1 || C > 16 || (ndim != 2 && ndim != 3)) return 0;
+  switch (padded(C) * 10 + static_cast<int>(ndim)) {
+#define X(CP, NS) \
+  case CP * 10 + NS: \
+    return Regs<CP, NS>::MINB;
+    PGB_TC_DISPATCH(X)
+#undef X
+    default:
+      return 0;
+  }
+}
+
+int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const void* wfrag, const void* dtab,
+                     int64_t nsteps, int64_t ndim, int64_t C, int64_t B, int64_t terms, const pgb_v6_plan* plan,
+                     void* stream) {
+  const char* who = "grog_grid_tc";
+  clear_error();
+  Geom geom;
+  int st = geom_of(plan, geom, who);
+  if (st) return st;
+  st = check_common(who, C, N, B, nsteps, ndim, terms, wfrag, dtab);
+  if (st) return st;
+  PGB_REQUIRE(G == static_cast<int64_t>(plan->gz) * plan->gy * plan->gx, PGB_ERR_INVALID,
+              "%s: G does not match the plan grid", who);
+  PGB_REQUIRE(ndim == 3 || plan->gz == 1, PGB_ERR_INVALID, "%s: a 2-D table needs a 2-D plan", who);
+  if (B == 0 || G == 0) return PGB_OK;
+  PGB_REQUIRE(grid && (data || N == 0), PGB_ERR_INVALID, "%s: null pointer", who);
+  const int cells = plan->bz * plan->by * plan->bx;
+  const size_t smem = pgb_grog_tc_smem_bytes(C, cells, nsteps, ndim, plan->sub_cap);
+  PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED, "%s: tile + staging need %zu B of shared memory", who, smem);
+  cudaStream_t s = as_stream(stream);
+  if (plan->n_zero_bricks > 0) {
+    PGB_REQUIRE(plan->zero_bricks != nullptr, PGB_ERR_INVALID, "%s: null zero-brick list", who);
+    const int64_t tot = static_cast<int64_t>(plan->n_zero_bricks) * cells;
+    zero_bricks_tc<<<grid_for(tot, 256, 148 * 16), 256, 0, s>>>(static_cast<float2*>(grid), G, static_cast<int>(C),
+                                                               static_cast<int>(B), plan->zero_bricks,
+                                                               plan->n_zero_bricks, geom);
+    PGB_LAUNCH_CHECK(who);
+  }
+  if (plan->n_cta == 0) return PGB_OK;
+  dim3 grd(plan->n_cta, static_cast<unsigned>(B));
+  const int key = padded(C) * 10 + static_cast<int>(ndim);
+  switch (key) {
+#define X(CP, NS)                                                                                               \
+  case CP * 10 + NS: {                                                                                          \
+    auto k = terms == 3 ? grog_grid_tc_kernel<CP, NS, 3> : grog_grid_tc_kernel<CP, NS, 1>;                      \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
+    k<<<grd, kT, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,                 \
+                            static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \
+                            static_cast<const float2*>(dtab), static_cast<int>(nsteps),                         \
+                            reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),    \
+                            plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,       \
+                            plan->sub_cap, geom);                                                               \
+  } break;
+    PGB_TC_DISPATCH(X)
+#undef X
+    default:
+      PGB_REQUIRE(false, PGB_ERR_UNSUPPORTED, "%s: no kernel for C=%lld ndim=%lld", who, (long long)C,
+                  (long long)ndim);
+  }
+  PGB_LAUNCH_CHECK(who);
+  return PGB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int degrid_tc_one(const char* who, const void* grid, int64_t G, void* out, int64_t N, const void* wfrag,
+                  const void* dtab, int64_t nsteps, int64_t ndim, int64_t C, int64_t B, int64_t terms,
+                  const pgb_v6_plan* plan, const Geom& geom, bool acc, cudaStream_t s) {
+  if (plan->n_cta == 0) return PGB_OK;
+  const int cells = plan->bz * plan->by * plan->bx;
+  const size_t smem = pgb_grog_tc_smem_bytes(C, cells, nsteps, ndim, plan->sub_cap);
+  PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED, "%s: tiles + results need %zu B of shared memory", who, smem);
+  dim3 grd(plan->n_cta, static_cast<unsigned>(B));
+  const int key = padded(C) * 10 + static_cast<int>(ndim);
+  switch (key) {
+#define X(CP, NS)                                                                                               \
+  case CP * 10 + NS: {                                                                                          \
+    auto k = terms == 3 ? (acc ? grog_degrid_tc_kernel<CP, NS, 3, true> : grog_degrid_tc_kernel<CP, NS, 3, false>) \
+                        : (acc ? grog_degrid_tc_kernel<CP, NS, 1, true> : grog_degrid_tc_kernel<CP, NS, 1, false>); \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
+    k<<<grd, kT, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                  \
+                            static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \
+                            static_cast<const float2*>(dtab), static_cast<int>(nsteps),                         \
+                            reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),    \
+                            plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,       \
+                            plan->sub_cap, geom);                                                               \
+  } break;
+    PGB_TC_DISPATCH(X)
+#undef X
+    default:
+      PGB_REQUIRE(false, PGB_ERR_UNSUPPORTED, "%s: no kernel for C=%lld ndim=%lld", who, (long long)C,
+                  (long long)ndim);
+  }
+  PGB_LAUNCH_CHECK(who);
+  return PGB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N, const void* wfrag_h, const void* dtab_h,
+                       int64_t nsteps, int64_t ndim, int64_t C, int64_t B, int64_t terms,
+                       const pgb_v6_plan* primary, const pgb_v6_plan* secondary, const int32_t* zero_src,
+                       int64_t n_zero, void* stream) {
+  const char* who = "grog_degrid_tc";
+  clear_error();
+  Geom geom;
+  int st = geom_of(primary, geom, who);
+  if (st) return st;
+  Geom g2;
+  if (secondary != nullptr) {
+    st = geom_of(secondary, g2, who);
+    if (st) return st;
+    PGB_REQUIRE(secondary->bz == primary->bz && secondary->by == primary->by && secondary->bx == primary->bx &&
+                    secondary->gz == primary->gz && secondary->gy == primary->gy && secondary->gx == primary->gx,
+                PGB_ERR_INVALID, "%s: primary and secondary plans differ in geometry", who);
+  }
+  st = check_common(who, C, N, B, nsteps, ndim, terms, wfrag_h, dtab_h);
+  if (st) return st;
+  PGB_REQUIRE(n_zero >= 0 && (n_zero == 0 || zero_src != nullptr), PGB_ERR_INVALID, "%s: bad zero-sample list",
+              who);
+  PGB_REQUIRE(G == static_cast<int64_t>(primary->gz) * primary->gy * primary->gx, PGB_ERR_INVALID,
+              "%s: G does not match the plan grid", who);
+  PGB_REQUIRE(ndim == 3 || primary->gz == 1, PGB_ERR_INVALID, "%s: a 2-D table needs a 2-D plan", who);
+  if (B == 0 || N == 0) return PGB_OK;
+  PGB_REQUIRE(out && grid, PGB_ERR_INVALID, "%s: null pointer", who);
+  cudaStream_t s = as_stream(stream);
+  st = degrid_tc_one(who, grid, G, out, N, wfrag_h, dtab_h, nsteps, ndim, C, B, terms, primary, geom, false, s);
+  if (st) return st;
+  if (secondary != nullptr) {
+    st = degrid_tc_one(who, grid, G, out, N, wfrag_h, dtab_h, nsteps, ndim, C, B, terms, secondary, g2, true, s);
+    if (st) return st;
+  }
+  if (n_zero > 0) {
+    zero_samples_tc<<<grid_for(n_zero * C * B, 256), 256, 0, s>>>(static_cast<float2*>(out), N, static_cast<int>(C),
+                                                                  static_cast<int>(B), zero_src, n_zero);
+    PGB_LAUNCH_CHECK(who);
+  }
+  return PGB_OK;
+}
+
+}  // extern "C"

@@ -161,3 +161,34 @@ def test_hot_brick_split_and_repeatability(cuda):
     back = g.degrid(a)
     refa = og.degrid(a.reshape(1, C, -1), g._interp_idx.cpu().numpy(), table, p)[0]
     assert rel_l2(back.reshape(C, -1), refa) < 1e-5
+
+
+@pytest.mark.parametrize("mode", ["tc", "tc1"])
+@pytest.mark.parametrize("ndim,n,spokes,readout,C,osf,kwd,ks,prec,B", [
+    (2, 64, 40, 128, 8, 1.0, 5, "square", 2, 1),   # c0-like: 501 steps, one valid replica
+    (2, 48, 30, 96, 16, 2.0, 2, "circle", 1, 2),   # several valid replicas (secondary plan), batch 2
+    (3, 24, 300, 48, 12, 1.0, 2, "sphere", 1, 1),  # c1-like kooshball
+    (2, 40, 20, 80, 5, 1.5, 3, "cross", 1, 1),     # odd coil count (padded to 8)
+    (3, 16, 200, 32, 4, 2.0, 2, "sphere", 1, 1),   # 4 coils, many replicas per cell
+])
+def test_tensor_core_grid_degrid_vs_fp64_oracle(cuda, ndim, n, spokes, readout, C, osf, kwd, ks, prec, B, mode):
+    """bf16x3 ("tc") within 1e-4 of the FP64 oracle; plain bf16 ("tc1") within 2e-2."""
+    coords, calib, data = _random_case(ndim, n, spokes, readout, C, osf, kwd, ks, prec, seed=n + C, B=B)
+    g = GrogInterpolator(shape=(n,) * ndim, coords=coords, oversamp=osf, kernel_width=kwd,
+                         kernel_shape=ks, device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=prec)
+    g.gridder_mode = mode
+    table = g._interp_kernel.numpy().astype(np.complex128)
+    p = og.create_plan((n,) * ndim, coords, osf, kwd, ks)
+    qi = g._interp_idx.cpu().numpy()
+    G = int(np.prod(p["grid_shape"]))
+    tol = 1e-4 if mode == "tc" else 2e-2
+    kg = g.grid(data)
+    assert g._brick(0).mode == mode
+    ref, _ = og.grid(data.reshape(B, C, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
+    assert rel_l2(kg.reshape(B, C, G), ref) < tol
+    out = g.degrid(kg)
+    ref_a = og.degrid(np.asarray(kg).reshape(B, C, G).astype(np.complex128), qi, table, p)
+    assert rel_l2(out.reshape(B, C, -1), ref_a) < tol
+    # repeat: same result (the shared tile / result buffers are re-zeroed)
+    assert rel_l2(g.grid(data), kg) < 1e-6
