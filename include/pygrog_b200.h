@@ -345,8 +345,12 @@ PGB_API int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N
  * down to even + (CP/4) % 2), CP = C rounded up to a multiple of 4; dtab:
  * complex64 (ndim, nsteps, CP) diagonal phases in application order.  terms: 3
  * = bf16x3 split products (~1e-5 relative), 1 = plain bf16.  Plans: v6 plans
- * built with n_outer = nsteps (meta.y = (e / nsteps) | (e % nsteps) << 16),
- * sub_cap <= 256; C <= 16.  The plan's n_cta should be 148 x
+ * built with n_outer = nsteps,
+ * sub_cap <= 256, meta.y = the per-axis shift indices (3-D i | j << 8 | k << 16
+ * with e = (i nsteps + j) nsteps + k and nsteps <= 255; 2-D i | k << 16 with
+ * e = i nsteps + k); the forward plan in (cell, sample) order inside each
+ * sub-chunk with meta.x bit 30 set on cells whose run crosses a 16-entry
+ * boundary; C <= 16.  The plan's n_cta should be 148 x
  * pgb_grog_tc_blocks_per_sm(C, ndim).  Same zeroing / primary / secondary /
  * zero_src contract as pgb_grog_grid_v6 / pgb_grog_degrid_v6. */
 PGB_API size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t ndim, int64_t sub_cap);

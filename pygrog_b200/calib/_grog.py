@@ -443,6 +443,22 @@ def _first_valid_mask(target_idx: torch.Tensor, kw: int) -> torch.Tensor:
     return (m & valid).reshape(-1)
 
 
+def _pack_axis_indices(bp: BrickPlan6, nsteps: int, ndim: int) -> None:
+    """Rewrite ``meta.y = q | k << 16`` (``e = q * nsteps + k``) of a v6 plan as
+    the per-axis shift indices the tensor-core kernels read: ``i | j << 8 |
+    k << 16`` in 3-D (``q = i * nsteps + j``, ``nsteps <= 255``), ``i | k << 16``
+    in 2-D."""
+    if ndim == 3 and nsteps > 255:
+        raise ValueError("tc kernels: 3-D tables need nsteps <= 255")
+    if bp.meta.numel() == 0:
+        return
+    y = bp.meta[:, 1].to(torch.int64)
+    q, k = y & 0xFFFF, y >> 16
+    if ndim == 3:
+        y = (q // nsteps) | ((q % nsteps) << 8) | (k << 16)
+    bp.meta[:, 1] = y.to(torch.int32)
+
+
 class GrogGridder:
     """Fused GROG gridding operator for one trajectory: brick plans + tables.
 
@@ -674,12 +690,15 @@ class GrogGridder:
         self.pairs = False
         dev = target_idx.device
         kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True)
-        self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, **kwt)
+        self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_rows=True, **kwt)
         first = _first_valid_mask(target_idx, kw)
         self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwt)
         self.plan2 = None
         if self.plan.n_valid > self.adj_plan.n_valid:
             self.plan2 = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kwt)
+        for bp in (self.plan, self.adj_plan, self.plan2):
+            if bp is not None:
+                _pack_axis_indices(bp, nsteps, nd)
 
     @property
     def n_valid(self):

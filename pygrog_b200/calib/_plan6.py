@@ -74,6 +74,7 @@ class BrickPlan6:
         seg_len: int = 8,
         pair_lanes: bool = False,
         sample_order: bool = False,
+        cell_rows: bool = False,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -177,6 +178,27 @@ class BrickPlan6:
             src = spread(src, -1)
             cl = spread(cl, cells)  # padding: no cell
             sub_id = sub_full
+        elif cell_rows and n:
+            # tensor-core forward: each sub-chunk in (cell, sample) order, so an
+            # m-tile's 16 rows hold runs of one cell that the kernel sums in
+            # registers; bit 30 of meta.x marks replicas of a cell whose run
+            # crosses an m-tile boundary (those segments are added atomically)
+            _, p2 = torch.sort((sub_id * cells + cl) * n_src + src, stable=True)
+            sub_id, cl, slot, q, k, w, src = (a[p2] for a in (sub_id, cl, slot, q, k, w, src))
+            rc = torch.bincount(sub_id, minlength=n_subs)
+            rb = torch.cumsum(rc, 0) - rc
+            pos = torch.arange(n, device=dev) - rb[sub_id]
+            head = torch.ones(n, dtype=torch.bool, device=dev)
+            head[1:] = (cl[1:] != cl[:-1]) | (sub_id[1:] != sub_id[:-1])
+            run_id = torch.cumsum(head.to(torch.int64), 0) - 1
+            run_len = torch.bincount(run_id)
+            run_pos = pos[head]
+            rs = run_pos[run_id]
+            re = rs + run_len[run_id] - 1
+            straddle = (rs // 16) != (re // 16)
+            self.meta = torch.stack([cl | (slot << 16) | (straddle.to(torch.int64) << 30), q | (k << 16)],
+                                    dim=1).to(torch.int32).contiguous()
+            self.w = w.contiguous()
         elif sample_order:
             # keep step (1)'s sample order: the tensor-core gridder reads each
             # m-tile's staged samples in order (conflict-free) and spreads

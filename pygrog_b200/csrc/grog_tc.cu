@@ -23,16 +23,20 @@
 // bf16 tail (x = hi + lo) and each product is hi*hi + hi*lo + lo*hi with fp32
 // accumulation (~2^-16 relative per stage); terms == 1 uses the heads only.
 //
-// Plans: the v6 brick plans (calib/_plan6.py) with n_outer = nsteps, i.e.
-// meta.y = q | k << 16 with q = e / nsteps and k = e % nsteps; in 3-D the
-// axis indices are (i, j, k) = (q / nsteps, q % nsteps, k), in 2-D (q, k).
-// Any replica order inside a sub-chunk is correct (sample order keeps the
-// staged-sample reads conflict-free).
+// Plans: the v6 brick plans (calib/_plan6.py) with the table index e split
+// into its per-axis shift indices, meta.y = i | j << 8 | k << 16 in 3-D
+// (e = (i nsteps + j) nsteps + k, nsteps <= 255) and i | k << 16 in 2-D
+// (e = i nsteps + k).
+// The forward plan orders each sub-chunk by (cell, sample) and marks cells
+// whose run crosses an m-tile boundary (meta.x bit 30); the adjoint plans keep
+// sample order (conflict-free result writes).
 //
 //   forward:  per sub-chunk, stage the samples' coils (cp.async, double
-//             buffered), run the chain for 16 replicas per warp, add w * y to
-//             the brick tile with shared atomics; flush the tile once per
-//             brick (global atomics only for bricks split over CTAs)
+//             buffered), run the chain for 16 replicas per warp, sum each
+//             cell's rows in registers (segmented scan over the m-tile) and
+//             add the totals to the brick tile (plain read-modify-writes;
+//             atomics only for runs crossing an m-tile); flush the tile once
+//             per brick (global atomics only for bricks split over CTAs)
 //   adjoint:  tile of the brick (cp.async, prefetched one brick ahead), the
 //             adjoint chain W3^H conj(Dx) W2^H conj(Dy) W1^H conj(Dz) W0^H per
 //             replica, w * y into a per-slot result buffer, flushed per
@@ -92,6 +96,10 @@ __device__ __forceinline__ void cp8(void* smem_dst, const void* gsrc, int bytes)
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void cp4(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void wait_groups() {
@@ -145,26 +153,34 @@ __device__ __forceinline__ void mm_stage(float2 (&v)[2][Shape<CP>::NT], const ui
   }
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    // products alternate between two accumulators (tails first): two short
+    // dependency chains instead of one long one
+    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
     int f = nt * (2 * K16 + K8);
+    int q = 0;
 #pragma unroll
     for (int kc = 0; kc < K16; ++kc) {
       if constexpr (TERMS == 3) {
-        mma16(d, al[0][2 * kc], al[1][2 * kc], al[0][2 * kc + 1], al[1][2 * kc + 1], bh[f], bh[f + 1]);
-        mma16(d, ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bl[f], bl[f + 1]);
+        mma16(d[q & 1], al[0][2 * kc], al[1][2 * kc], al[0][2 * kc + 1], al[1][2 * kc + 1], bh[f], bh[f + 1]);
+        ++q;
+        mma16(d[q & 1], ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bl[f], bl[f + 1]);
+        ++q;
       }
-      mma16(d, ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bh[f], bh[f + 1]);
+      mma16(d[q & 1], ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bh[f], bh[f + 1]);
+      ++q;
       f += 2;
     }
     if constexpr (K8) {
       if constexpr (TERMS == 3) {
-        mma8(d, al[0][NT - 1], al[1][NT - 1], bh[f]);
-        mma8(d, ah[0][NT - 1], ah[1][NT - 1], bl[f]);
+        mma8(d[q & 1], al[0][NT - 1], al[1][NT - 1], bh[f]);
+        ++q;
+        mma8(d[q & 1], ah[0][NT - 1], ah[1][NT - 1], bl[f]);
+        ++q;
       }
-      mma8(d, ah[0][NT - 1], ah[1][NT - 1], bh[f]);
+      mma8(d[q & 1], ah[0][NT - 1], ah[1][NT - 1], bh[f]);
     }
-    v[0][nt] = make_float2(d[0], d[1]);
-    v[1][nt] = make_float2(d[2], d[3]);
+    v[0][nt] = make_float2(d[0][0] + d[1][0], d[0][1] + d[1][1]);
+    v[1][nt] = make_float2(d[0][2] + d[1][2], d[0][3] + d[1][3]);
   }
 }
 
@@ -185,35 +201,26 @@ __device__ __forceinline__ void load_w(const uint32_t* __restrict__ wfrag, int l
 struct Row {
   int cell, slot, ix0, ix1, ix2;
   float w;
-  bool on;
+  bool on, straddle;
 };
 
 template <int NS>
 __device__ __forceinline__ Row decode(int2 m, float w, bool in_range, int cells, int nu, int nsteps) {
   Row r;
   r.cell = m.x & 0xFFFF;
-  r.slot = static_cast<int>(static_cast<unsigned>(m.x) >> 16);
-  const int q = m.y & 0xFFFF;
-  const int k = static_cast<int>(static_cast<unsigned>(m.y) >> 16);
-  const int nq = NS == 3 ? nsteps * nsteps : nsteps;
-  r.on = in_range && m.x >= 0 && r.cell < cells && r.slot < nu && q < nq && k < nsteps;
-  if (!r.on) {
-    r.cell = 0;
-    r.slot = 0;
-    r.ix0 = r.ix1 = r.ix2 = 0;
-    r.w = 0.f;
-    return r;
-  }
-  if constexpr (NS == 3) {
-    r.ix0 = q / nsteps;
-    r.ix1 = q - r.ix0 * nsteps;
-    r.ix2 = k;
-  } else {
-    r.ix0 = q;
-    r.ix1 = k;
-    r.ix2 = 0;
-  }
-  r.w = w;
+  r.slot = (m.x >> 16) & 0x3FFF;
+  r.straddle = (m.x >> 30) & 1;
+  // axis indices packed by the plan: 3-D i | j << 8 | k << 16, 2-D i | k << 16
+  const int a0 = NS == 3 ? (m.y & 0xFF) : (m.y & 0xFFFF);
+  const int a1 = NS == 3 ? ((m.y >> 8) & 0xFF) : ((m.y >> 16) & 0xFFFF);
+  const int a2 = NS == 3 ? ((m.y >> 16) & 0xFFFF) : 0;
+  r.on = in_range && m.x >= 0 && r.cell < cells && r.slot < nu && a0 < nsteps && a1 < nsteps && a2 < nsteps;
+  r.ix0 = r.on ? a0 : 0;
+  r.ix1 = r.on ? a1 : 0;
+  r.ix2 = r.on ? a2 : 0;
+  r.cell = r.on ? r.cell : 0;
+  r.slot = r.on ? r.slot : 0;
+  r.w = r.on ? w : 0.f;
   return r;
 }
 
@@ -227,7 +234,8 @@ __device__ __forceinline__ int diag_index(const Row& r, int s) {
 // of table dt (NS, nsteps, CP) between them.
 template <int CP, int NS, int TERMS, bool ADJ>
 __device__ __forceinline__ void chain(float2 (&v)[2][Shape<CP>::NT], const uint32_t (&wb)[NS + 1][2][Shape<CP>::NFR],
-                                      const float2* __restrict__ dt, int nsteps, const Row (&rw)[2], int t) {
+                                      const float2* __restrict__ dt, int nsteps, int dstride, const Row (&rw)[2],
+                                      int t) {
   constexpr int NT = Shape<CP>::NT;
 #pragma unroll
   for (int s = 0; s <= NS; ++s) {
@@ -235,7 +243,7 @@ __device__ __forceinline__ void chain(float2 (&v)[2][Shape<CP>::NT], const uint3
     if (s < NS) {
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
-        const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[r], s)) * CP + t;
+        const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[r], s)) * dstride + t;
 #pragma unroll
         for (int m = 0; m < NT; ++m) v[r][m] = cmul(v[r][m], drow[4 * m]);
       }
@@ -276,43 +284,162 @@ struct Stream {
 __device__ __forceinline__ int n_slots(int4 d, int cap) { return min(max(d.w - d.z, 0), cap); }
 __device__ __forceinline__ int n_reps(int4 d, int cap) { return min(max(d.y - d.x, 0), cap); }
 
-// Metadata of this lane's four rows (two m-tiles x rows g, g + 8) of sub-chunk d.
-struct LaneMeta {
-  int2 m[2][2];
-  float w[2][2];
-};
-__device__ __forceinline__ void load_meta(LaneMeta& lm, const int2* __restrict__ meta, const float* __restrict__ wts,
-                                          int4 d, bool valid, int cap, int warp, int g) {
-  const int nr = valid ? n_reps(d, cap) : 0;
-#pragma unroll
-  for (int j = 0; j < 2; ++j)
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int row = (warp + 8 * j) * 16 + 8 * r + g;
-      if (row < nr) {
-        lm.m[j][r] = __ldg(meta + d.x + row);
-        lm.w[j][r] = __ldg(wts + d.x + row);
-      } else {
-        lm.m[j][r] = make_int2(-1, 0);
-        lm.w[j][r] = 0.f;
-      }
-    }
+// Stage the replica metadata and weights of sub-chunk d (cp.async).
+__device__ __forceinline__ void stage_meta(const int2* __restrict__ meta, const float* __restrict__ wts, int4 d,
+                                           int cap, int2* __restrict__ ms, float* __restrict__ wsm) {
+  const int nr = n_reps(d, cap);
+  for (int i = threadIdx.x; i < nr; i += kT) {
+    cp8(ms + i, meta + d.x + i, 8);
+    cp4(wsm + i, wts + d.x + i);
+  }
 }
 
-// Shared-memory layout in float2 units: diagonal tables | tile(s) | staging (x or results)
-struct Smem {
-  int dt, tile, tile_sz, xs, xs_sz, total;
-  __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward) {
-    dt = 0;
-    tile = (NS * nsteps * CP + 1) & ~1;
-    tile_sz = (cells * (CP + 1) + 1) & ~1;
-    xs = tile + (forward ? 1 : 2) * tile_sz;
-    xs_sz = CP * (cap + 4);
-    total = xs + (forward ? 2 : 1) * xs_sz;
+// Phase tables in shared memory: with 4 copies every step row is 16 float2
+// (64 words, bank-aligned) and copy k starts 8 k words into the bank cycle,
+// so the quarter-warps of rows g = 0..3 (copy g % 4) read disjoint banks
+// whatever their shift indices; with 1 copy rows are CP float2.
+struct Phases {
+  int copies, stride, copy_sz;
+  __host__ __device__ Phases(int CP, int NS, int nsteps) {
+    const int sz4 = NS * nsteps * 16 + 4;
+    if (CP <= 16 && 4 * sz4 * 8 <= 32 * 1024) {
+      copies = 4;
+      stride = 16;
+      copy_sz = sz4;
+    } else {
+      copies = 1;
+      stride = CP;
+      copy_sz = NS * nsteps * CP;
+    }
   }
 };
 
-template <int CP, int NS, int TERMS>
+// Shared-memory layout in float2 units: phase tables | tile(s) | staging (x or results)
+struct Smem {
+  int dt, tile, tile_sz, xs, xs_sz, ms, wsm, total;
+  __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward) {
+    dt = 0;
+    const Phases ph(CP, NS, nsteps);
+    tile = (ph.copies * ph.copy_sz + 1) & ~1;
+    tile_sz = (cells * (CP + 1) + 1) & ~1;
+    xs = tile + (forward ? 1 : 2) * tile_sz;
+    xs_sz = CP * (cap + 4);
+    ms = xs + (forward ? 2 : 1) * xs_sz;  // 2 x cap replica metadata (int2)
+    wsm = ms + 2 * cap;                   // 2 x cap replica weights (float)
+    total = wsm + cap;
+  }
+};
+
+// Copy the (NS, nsteps, CP) phase table into its shared-memory copies.
+__device__ __forceinline__ void stage_phases(float2* __restrict__ dt, const float2* __restrict__ dtab, int CP, int NS,
+                                             int nsteps, const Phases& ph) {
+  const int n = NS * nsteps * CP;
+  for (int i = threadIdx.x; i < ph.copies * n; i += kT) {
+    const int cp = i / n;
+    const int e = i - cp * n;
+    const int row = e / CP;
+    dt[cp * ph.copy_sz + row * ph.stride + (e - row * CP)] = __ldg(dtab + e);
+  }
+}
+
+// Sum the rows of one m-tile that belong to the same cell and add each cell's
+// sum to the brick tile.  Rows hold sub-chunk positions p = 2 g + r in cell
+// order (row g + 8 r of lane group g), so a cell is a run of consecutive
+// positions: the pair of a lane is combined in registers, runs across lane
+// groups by a segmented inclusive scan over g (shuffles by 4, 8, 16 lanes),
+// and the last position of every run adds the total to tile[cell].  Runs
+// that do not cross the m-tile (straddle bit clear) have no other writer in
+// the sub-chunk and use plain read-modify-writes; the others add atomically.
+template <int CP, bool FULLC>
+__device__ __forceinline__ void reduce_rows_to_tile(float2 (&v)[2][Shape<CP>::NT], const Row (&rw)[2], int C,
+                                                    float2* __restrict__ tile, int g, int t) {
+  constexpr int NT = Shape<CP>::NT, TS = Shape<CP>::TS;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int k0 = rw[0].on ? rw[0].cell : -1 - 2 * g;  // invalid rows: unique keys, never written
+  const int k1 = rw[1].on ? rw[1].cell : -2 - 2 * g;
+  int kprev = __shfl_up_sync(FULL, k1, 4);    // cell of position 2 g - 1
+  int knext = __shfl_down_sync(FULL, k0, 4);  // cell of position 2 g + 2
+  if (g == 0) kprev = -100;
+  if (g == 7) knext = -101;
+  const bool pair = k1 == k0;
+  if (!__any_sync(FULL, pair || k0 == kprev)) {  // 16 distinct cells: no sums across rows
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (!rw[r].on) continue;
+      float2* dst = tile + rw[r].cell * TS;
+#pragma unroll
+      for (int m = 0; m < NT; ++m) {
+        const int c = 4 * m + t;
+        if (!FULLC && c >= C) continue;
+        if (rw[r].straddle) {
+          atomicAdd(&dst[c].x, v[r][m].x);
+          atomicAdd(&dst[c].y, v[r][m].y);
+        } else {
+          dst[c] = cadd(dst[c], v[r][m]);
+        }
+      }
+    }
+    return;
+  }
+  float2 a[NT];
+#pragma unroll
+  for (int m = 0; m < NT; ++m) a[m] = pair ? cadd(v[1][m], v[0][m]) : v[1][m];
+  bool open = pair && k0 == kprev;  // position 2 g + 1's run continues into lane group g - 1
+#pragma unroll
+  for (int off = 1; off < 8; off <<= 1) {
+    float2 ap[NT];
+#pragma unroll
+    for (int m = 0; m < NT; ++m) {
+      ap[m].x = __shfl_up_sync(FULL, a[m].x, 4 * off);
+      ap[m].y = __shfl_up_sync(FULL, a[m].y, 4 * off);
+    }
+    const bool op = __shfl_up_sync(FULL, open ? 1 : 0, 4 * off) != 0;
+    if (g >= off && open) {
+#pragma unroll
+      for (int m = 0; m < NT; ++m) a[m] = cadd(a[m], ap[m]);
+      open = op;
+    }
+  }
+  float2 aprev[NT];  // scanned run total up to position 2 g - 1
+#pragma unroll
+  for (int m = 0; m < NT; ++m) {
+    aprev[m].x = __shfl_up_sync(FULL, a[m].x, 4);
+    aprev[m].y = __shfl_up_sync(FULL, a[m].y, 4);
+  }
+  // position 2 g ends a run when 2 g + 1 holds another cell
+  if (!pair && rw[0].on) {
+    const bool carry = k0 == kprev;
+    float2* dst = tile + rw[0].cell * TS;
+#pragma unroll
+    for (int m = 0; m < NT; ++m) {
+      const int c = 4 * m + t;
+      if (!FULLC && c >= C) continue;
+      const float2 val = carry ? cadd(v[0][m], aprev[m]) : v[0][m];
+      if (rw[0].straddle) {
+        atomicAdd(&dst[c].x, val.x);
+        atomicAdd(&dst[c].y, val.y);
+      } else {
+        dst[c] = cadd(dst[c], val);
+      }
+    }
+  }
+  if (k1 != knext && rw[1].on) {
+    float2* dst = tile + rw[1].cell * TS;
+#pragma unroll
+    for (int m = 0; m < NT; ++m) {
+      const int c = 4 * m + t;
+      if (!FULLC && c >= C) continue;
+      if (rw[1].straddle) {
+        atomicAdd(&dst[c].x, a[m].x);
+        atomicAdd(&dst[c].y, a[m].y);
+      } else {
+        dst[c] = cadd(dst[c], a[m]);
+      }
+    }
+  }
+}
+
+template <int CP, int NS, int TERMS, bool FULLC>
 __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G, int C,
     const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
@@ -324,52 +451,63 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
   if (p0 >= p1) return;  // block-uniform
   const int cells = geom.bz * geom.by * geom.bx;
   const Smem lay(CP, NS, nsteps, cells, cap, true);
+  const Phases ph(CP, NS, nsteps);
   const int XS = cap + 4;
   float2* base = reinterpret_cast<float2*>(smem4);
   float2* dt = base + lay.dt;
   float2* tile = base + lay.tile;
   float2* xs0 = base + lay.xs;
+  int2* ms0 = reinterpret_cast<int2*>(base + lay.ms);
+  float* ws0 = reinterpret_cast<float*>(base + lay.wsm);
   const int b = blockIdx.y;
   const float2* dat = data + static_cast<int64_t>(b) * C * N;
   float2* grd = grid + static_cast<int64_t>(b) * C * G;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const float2* dtl = dt + (ph.copies == 4 ? (g & 3) * ph.copy_sz : 0);  // this lane's phase copy
 
-  auto stage_x = [&](int4 d, float2* xs) {  // samples' coils of sub-chunk d, coil-major
+  auto ld_u = [&](int4 d, bool valid) -> int {
+    return (valid && tid < n_slots(d, cap)) ? __ldg(uniq + d.z + tid) : -1;
+  };
+  auto stage_x = [&](int4 d, int u, float2* xs) {  // samples' coils of sub-chunk d, coil-major
     const int nu = n_slots(d, cap);
     if (tid < nu) {
-      const int u = __ldg(uniq + d.z + tid);
       const bool ok = u >= 0 && u < N;
-      for (int c = 0; c < C; ++c)
-        cp8(xs + c * XS + tid, ok ? dat + static_cast<int64_t>(c) * N + u : dat, ok ? 8 : 0);
+      const float2* src = ok ? dat + u : dat;
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (FULLC || c < C) cp8(xs + c * XS + tid, ok ? src + static_cast<int64_t>(c) * N : dat, ok ? 8 : 0);
     }
   };
 
   Stream st;
   st.init(sd, si, p0, p1);
-  stage_x(st.d0, xs0);
+  stage_x(st.d0, ld_u(st.d0, true), xs0);
+  stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
+  int u1 = ld_u(st.d1, st.p + 1 < p1);  // staging slots of the next sub-chunk, one iteration ahead
   uint32_t wb[NS + 1][2][NFR];
   load_w<CP, NS>(wfrag, lane, wb);
-  for (int i = tid; i < NS * nsteps * CP; i += kT) dt[i] = __ldg(dtab + i);
+  stage_phases(dt, dtab, CP, NS, nsteps, ph);
   for (int i = tid; i < lay.tile_sz; i += kT) tile[i] = make_float2(0.f, 0.f);
-  LaneMeta lm, ln;
-  load_meta(lm, meta, wts, st.d0, true, cap, warp, g);
 
   int buf = 0;
   while (true) {
     const bool more = st.p + 1 < p1;
     if (more) {
-      stage_x(st.d1, xs0 + (buf ^ 1) * lay.xs_sz);
+      stage_x(st.d1, u1, xs0 + (buf ^ 1) * lay.xs_sz);
+      stage_meta(meta, wts, st.d1, cap, ms0 + (buf ^ 1) * cap, ws0 + (buf ^ 1) * cap);
       commit();
       wait_groups<1>();
     } else {
       wait_groups<0>();
     }
-    load_meta(ln, meta, wts, st.d1, more, cap, warp, g);
+    const int u2 = ld_u(st.d2, st.p + 2 < p1);
     __syncthreads();  // staging buffer `buf` complete; tile zeroed / flushed
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
       const float2* xs = xs0 + buf * lay.xs_sz;
+      const int2* msb = ms0 + buf * cap;
+      const float* wsb = ws0 + buf * cap;
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int mt = warp + 8 * j;
@@ -378,27 +516,22 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
         float2 v[2][NT];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-          rw[r] = decode<NS>(lm.m[j][r], lm.w[j][r], mt * 16 + 8 * r + g < nr, cells, nu, nsteps);
+          const int e = mt * 16 + 2 * g + r;  // cell-ordered rows: entry 2 g + r on row g + 8 r
+          const bool in = e < nr;
+          rw[r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
 #pragma unroll
           for (int m = 0; m < NT; ++m) {
             const int c = 4 * m + t;
-            v[r][m] = (rw[r].on && c < C) ? xs[c * XS + rw[r].slot] : make_float2(0.f, 0.f);
+            v[r][m] = (rw[r].on && (FULLC || c < C)) ? xs[c * XS + rw[r].slot] : make_float2(0.f, 0.f);
           }
         }
-        chain<CP, NS, TERMS, false>(v, wb, dt, nsteps, rw, t);
+        chain<CP, NS, TERMS, false>(v, wb, dtl, nsteps, ph.stride, rw, t);
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          if (!rw[r].on) continue;
-          float2* dst = tile + rw[r].cell * TS;
+        for (int r = 0; r < 2; ++r)
 #pragma unroll
-          for (int m = 0; m < NT; ++m) {
-            const int c = 4 * m + t;
-            if (c < C) {
-              atomicAdd(&dst[c].x, rw[r].w * v[r][m].x);
-              atomicAdd(&dst[c].y, rw[r].w * v[r][m].y);
-            }
-          }
-        }
+          for (int m = 0; m < NT; ++m) v[r][m] = cscale(v[r][m], rw[r].w);
+        reduce_rows_to_tile<CP, FULLC>(v, rw, C, tile, g, t);
+        __syncwarp();
       }
     }
     __syncthreads();  // tile complete for this sub-chunk; staging buffer `buf` free
@@ -406,32 +539,38 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       int z0, y0, x0;
       origin(geom, st.i0.x, z0, y0, x0);
       const bool split = (st.i0.y & kSplit) != 0;
-      for (int i = tid; i < C * cells; i += kT) {
-        const int c = i / cells;
-        const int cl = i - c * cells;
-        const float2 v = tile[cl * TS + c];
-        tile[cl * TS + c] = make_float2(0.f, 0.f);  // this thread re-zeroes what it flushed
+      for (int cl = tid; cl < cells; cl += kT) {  // one cell per thread, all coils
         int64_t flat;
-        if (!flat_of(geom, z0, y0, x0, cl, flat)) continue;
-        float2* dst = grd + static_cast<int64_t>(c) * G + flat;
-        if (split) {
-          if (v.x != 0.f || v.y != 0.f) {
-            atomicAdd(&dst->x, v.x);
-            atomicAdd(&dst->y, v.y);
+        const bool in = flat_of(geom, z0, y0, x0, cl, flat);
+        float2* trow = tile + cl * TS;
+        float2* dst = grd + (in ? flat : 0);
+#pragma unroll
+        for (int c = 0; c < CP; ++c) {
+          if (!FULLC && c >= C) break;
+          const float2 v = trow[c];
+          trow[c] = make_float2(0.f, 0.f);  // this thread re-zeroes what it flushed
+          if (in) {
+            if (split) {
+              if (v.x != 0.f || v.y != 0.f) {
+                atomicAdd(&dst->x, v.x);
+                atomicAdd(&dst->y, v.y);
+              }
+            } else {
+              *dst = v;
+            }
           }
-        } else {
-          *dst = v;
+          dst += G;
         }
       }
     }
     if (!more) break;
     st.advance();
-    lm = ln;
+    u1 = u2;
     buf ^= 1;
   }
 }
 
-template <int CP, int NS, int TERMS, bool ACC>
+template <int CP, int NS, int TERMS, bool ACC, bool FULLC>
 __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     const float2* __restrict__ grid, int64_t G, float2* __restrict__ out, int64_t N, int C,
     const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
@@ -448,20 +587,25 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
   float2* dt = base + lay.dt;
   float2* tiles = base + lay.tile;  // 2 x (cells, TS)
   float2* res = base + lay.xs;      // (CP, XS) per-slot results
+  int2* ms0 = reinterpret_cast<int2*>(base + lay.ms);
+  float* ws0 = reinterpret_cast<float*>(base + lay.wsm);
+  const Phases ph(CP, NS, nsteps);
   const int b = blockIdx.y;
   const float2* grd = grid + static_cast<int64_t>(b) * C * G;
   float2* o = out + static_cast<int64_t>(b) * C * N;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const float2* dtl = dt + (ph.copies == 4 ? (g & 3) * ph.copy_sz : 0);  // this lane's phase copy
 
-  auto issue_tile = [&](int brick, float2* tl) {
+  auto issue_tile = [&](int brick, float2* tl) {  // one cell per thread, all coils
     int z0, y0, x0;
     origin(geom, brick, z0, y0, x0);
-    for (int i = tid; i < C * cells; i += kT) {
-      const int c = i / cells;
-      const int cl = i - c * cells;
+    for (int cl = tid; cl < cells; cl += kT) {
       int64_t flat;
       const bool in = flat_of(geom, z0, y0, x0, cl, flat);
-      cp8(tl + cl * TS + c, in ? grd + static_cast<int64_t>(c) * G + flat : grd, in ? 8 : 0);
+      const float2* src = grd + (in ? flat : 0);
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (FULLC || c < C) cp8(tl + cl * TS + c, in ? src + static_cast<int64_t>(c) * G : grd, in ? 8 : 0);
     }
   };
   auto ld_u = [&](int4 d, bool valid) -> int {
@@ -470,33 +614,34 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
 
   Stream st;
   st.init(sd, si, p0, p1);
-  int par = 0;
+  int par = 0, mb = 0;
   issue_tile(st.i0.x, tiles);
+  stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
   uint32_t wb[NS + 1][2][NFR];
   load_w<CP, NS>(wfrag, lane, wb);
-  for (int i = tid; i < NS * nsteps * CP; i += kT) dt[i] = __ldg(dtab + i);
+  stage_phases(dt, dtab, CP, NS, nsteps, ph);
   for (int i = tid; i < lay.xs_sz; i += kT) res[i] = make_float2(0.f, 0.f);
-  LaneMeta lm, ln;
-  load_meta(lm, meta, wts, st.d0, true, cap, warp, g);
   int u0 = ld_u(st.d0, true);
 
   while (true) {
     const bool more = st.p + 1 < p1;
     const bool last = (st.i0.y & kLast) != 0;
-    if (last && more) {  // next brick's tile into the other buffer during this compute
-      issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz);
+    if (more) {  // next sub-chunk's metadata (and next brick's tile) during this compute
+      if (last) issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz);
+      stage_meta(meta, wts, st.d1, cap, ms0 + (mb ^ 1) * cap, ws0 + (mb ^ 1) * cap);
       commit();
       wait_groups<1>();
     } else {
       wait_groups<0>();
     }
-    load_meta(ln, meta, wts, st.d1, more, cap, warp, g);
     const int u1 = ld_u(st.d1, more);
     __syncthreads();  // tile of this brick complete; previous results flushed
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
       const float2* tl = tiles + par * lay.tile_sz;
+      const int2* msb = ms0 + mb * cap;
+      const float* wsb = ws0 + mb * cap;
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int mt = warp + 8 * j;
@@ -505,21 +650,23 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
         float2 v[2][NT];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-          rw[r] = decode<NS>(lm.m[j][r], lm.w[j][r], mt * 16 + 8 * r + g < nr, cells, nu, nsteps);
+          const int e = mt * 16 + 8 * r + g;  // sample-ordered rows: entry 8 r + g on row g + 8 r
+          const bool in = e < nr;
+          rw[r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
 #pragma unroll
           for (int m = 0; m < NT; ++m) {
             const int c = 4 * m + t;
-            v[r][m] = (rw[r].on && c < C) ? tl[rw[r].cell * TS + c] : make_float2(0.f, 0.f);
+            v[r][m] = (rw[r].on && (FULLC || c < C)) ? tl[rw[r].cell * TS + c] : make_float2(0.f, 0.f);
           }
         }
-        chain<CP, NS, TERMS, true>(v, wb, dt, nsteps, rw, t);
+        chain<CP, NS, TERMS, true>(v, wb, dtl, nsteps, ph.stride, rw, t);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
           if (!rw[r].on) continue;
 #pragma unroll
           for (int m = 0; m < NT; ++m) {
             const int c = 4 * m + t;
-            if (c < C) {
+            if (FULLC || c < C) {
               float2* dst = res + c * XS + rw[r].slot;
               if (ACC) {
                 atomicAdd(&dst->x, rw[r].w * v[r][m].x);
@@ -535,24 +682,28 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     __syncthreads();  // results complete; this brick's tile no longer read
     if (tid < n_slots(st.d0, cap)) {
       const bool ok = u0 >= 0 && u0 < N;
-      for (int c = 0; c < C; ++c) {
+      float2* dst = o + (ok ? u0 : 0);
+#pragma unroll
+      for (int c = 0; c < CP; ++c) {
+        if (!FULLC && c >= C) break;
         float2* rv = res + c * XS + tid;
         const float2 v = *rv;
         if (ACC) *rv = make_float2(0.f, 0.f);  // this thread re-clears what it flushed
-        if (!ok) continue;
-        float2* dst = o + static_cast<int64_t>(c) * N + u0;
-        if (ACC) {
-          atomicAdd(&dst->x, v.x);
-          atomicAdd(&dst->y, v.y);
-        } else {
-          *dst = v;
+        if (ok) {
+          if (ACC) {
+            atomicAdd(&dst->x, v.x);
+            atomicAdd(&dst->y, v.y);
+          } else {
+            *dst = v;
+          }
         }
+        dst += N;
       }
     }
     if (!more) break;
     if (last) par ^= 1;
+    mb ^= 1;
     st.advance();
-    lm = ln;
     u0 = u1;
   }
 }
@@ -688,7 +839,9 @@ int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const v
   switch (key) {
 #define X(CP, NS)                                                                                               \
   case CP * 10 + NS: {                                                                                          \
-    auto k = terms == 3 ? grog_grid_tc_kernel<CP, NS, 3> : grog_grid_tc_kernel<CP, NS, 1>;                      \
+    const bool full = C == CP;                                                                                  \
+    auto k = terms == 3 ? (full ? grog_grid_tc_kernel<CP, NS, 3, true> : grog_grid_tc_kernel<CP, NS, 3, false>)    \
+                        : (full ? grog_grid_tc_kernel<CP, NS, 1, true> : grog_grid_tc_kernel<CP, NS, 1, false>);   \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
     k<<<grd, kT, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,                 \
                             static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \
@@ -723,8 +876,12 @@ int degrid_tc_one(const char* who, const void* grid, int64_t G, void* out, int64
   switch (key) {
 #define X(CP, NS)                                                                                               \
   case CP * 10 + NS: {                                                                                          \
-    auto k = terms == 3 ? (acc ? grog_degrid_tc_kernel<CP, NS, 3, true> : grog_degrid_tc_kernel<CP, NS, 3, false>) \
-                        : (acc ? grog_degrid_tc_kernel<CP, NS, 1, true> : grog_degrid_tc_kernel<CP, NS, 1, false>); \
+    const bool full = C == CP;                                                                                  \
+    auto k = terms == 3                                                                                         \
+                 ? (acc ? (full ? grog_degrid_tc_kernel<CP, NS, 3, true, true> : grog_degrid_tc_kernel<CP, NS, 3, true, false>)     \
+                        : (full ? grog_degrid_tc_kernel<CP, NS, 3, false, true> : grog_degrid_tc_kernel<CP, NS, 3, false, false>))  \
+                 : (acc ? (full ? grog_degrid_tc_kernel<CP, NS, 1, true, true> : grog_degrid_tc_kernel<CP, NS, 1, true, false>)     \
+                        : (full ? grog_degrid_tc_kernel<CP, NS, 1, false, true> : grog_degrid_tc_kernel<CP, NS, 1, false, false>)); \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
     k<<<grd, kT, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                  \
                             static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \

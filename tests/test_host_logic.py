@@ -330,3 +330,36 @@ def test_brick_plan6_cell_order_words():
             assert np.all(shared[s0:s0 + L] == (L > seg))
         n_shared += int(shared.sum())
     assert n_shared > 0  # the hot cells give runs longer than a segment
+
+
+def test_cell_row_plan_runs_and_straddle_bits():
+    """Tensor-core forward plan: (cell, sample) order inside each sub-chunk and
+    bit 30 of meta.x set exactly on runs that cross a 16-row m-tile."""
+    import torch
+
+    from pygrog_b200.calib._plan6 import BrickPlan6
+
+    rng = np.random.default_rng(3)
+    n_src, kw, gs = 3000, 1, (16, 32, 32)
+    tgt = torch.as_tensor(rng.integers(0, 16 * 32 * 32 // 64, (n_src, kw)) * 7 % (16 * 32 * 32))
+    tgt[::5] = 100  # a hot cell
+    idx = torch.as_tensor(rng.integers(0, 11 ** 3, (n_src, kw)))
+    w = torch.rand(n_src, kw)
+    p = BrickPlan6(tgt, idx, w, kw, gs, brick=(4, 8, 8), n_outer=11, sub_cap=256, n_cta=4, sample_order=True,
+                   cell_rows=True)
+    meta = p.meta.numpy()
+    cell = meta[:, 0] & 0xFFFF
+    strad = (meta[:, 0] >> 30) & 1
+    assert (meta[:, 0] >= 0).all()
+    for b, e, _, _ in p.subs.numpy():
+        c = cell[b:e]
+        assert (np.diff(c) >= 0).all()
+        for v in np.unique(c):
+            pos = np.nonzero(c == v)[0]
+            crosses = pos[0] // 16 != pos[-1] // 16
+            assert (strad[b:e][pos] == crosses).all()
+    # same replicas (cell, weight) as a sample-ordered plan
+    q = BrickPlan6(tgt, idx, w, kw, gs, brick=(4, 8, 8), n_outer=11, sub_cap=256, n_cta=4, sample_order=True)
+    assert p.n_valid == q.n_valid == n_src
+    assert sorted(zip(cell.tolist(), p.w.numpy().round(6).tolist())) == \
+        sorted(zip((q.meta.numpy()[:, 0] & 0xFFFF).tolist(), q.w.numpy().round(6).tolist()))
