@@ -178,6 +178,91 @@ def make_acr3d(device, seed: int):
     return (comp @ flat).reshape(N_COILS, 24, 24, 24).to(torch.complex64).numpy()
 
 
+class Fp64Check:
+    """FP64 restatement of the fused operator on the GPU (torch, complex128),
+    chunked over the valid replicas: grid[c, cell] += w * (T[e] x)_c and its
+    adjoint.  Used to report the relative L2 error of the measured path."""
+
+    def __init__(self, g, N: int, C: int):
+        import torch
+
+        plan = g.plan
+        self.kw = int(plan.target_idx.shape[-1])
+        self.tgt = plan.target_idx.reshape(-1)
+        sw = torch.sqrt(plan.weights.reshape(-1).clamp(min=0.0))
+        self.rw = (sw * sw).double()
+        self.idx = g._interp_idx.reshape(-1)
+        self.T = g._interp_kernel.to(self.tgt.device).to(torch.complex128)
+        self.valid = torch.nonzero(self.tgt >= 0).squeeze(1)
+        self.N, self.C = N, C
+        self.G = int(np.prod(plan.grid_shape))
+
+    def forward(self, x):
+        import torch
+
+        x = x.to(torch.complex128)
+        out = torch.zeros(self.C, self.G, dtype=torch.complex128, device=x.device)
+        for s in range(0, self.valid.numel(), 1 << 20):
+            r = self.valid[s:s + (1 << 20)]
+            y = torch.einsum("nrc,cn->rn", self.T[self.idx[r]], x[:, r // self.kw]) * self.rw[r]
+            out.index_add_(1, self.tgt[r], y)
+        return out
+
+    def adjoint(self, y):
+        import torch
+
+        y = y.to(torch.complex128)
+        out = torch.zeros(self.C, self.N, dtype=torch.complex128, device=y.device)
+        for s in range(0, self.valid.numel(), 1 << 20):
+            r = self.valid[s:s + (1 << 20)]
+            v = torch.einsum("nrc,rn->cn", self.T[self.idx[r]].conj(), y[:, self.tgt[r]]) * self.rw[r]
+            out.index_add_(1, r // self.kw, v)
+        return out
+
+    @staticmethod
+    def rel(a, b) -> float:
+        import torch
+
+        return float((a.to(torch.complex128) - b).norm() / b.norm())
+
+
+def time_modes(g, data, modes, ref_fwd, chk, reps: int = 6, warm: int = 3) -> dict:
+    """Forward / adjoint CUDA-event times and FP64 errors of several gridders."""
+    import torch
+
+    B, C, N = data.shape
+    G = int(np.prod(g.plan.grid_shape))
+    res = {}
+    saved = getattr(g, "gridder_mode", None)
+    for mode in modes:
+        g.gridder_mode = mode
+        g._brick_plans = None
+        bp = g._brick(0)
+        kg = torch.empty(B, C, G, dtype=torch.complex64, device=data.device)
+        out = torch.empty(B, C, N, dtype=torch.complex64, device=data.device)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        tf, ta = [], []
+        for it in range(warm + reps):
+            ev[0].record()
+            bp.forward(data, kg)
+            ev[1].record()
+            bp.adjoint(kg, out)
+            ev[2].record()
+            torch.cuda.synchronize()
+            if it >= warm:
+                tf.append(ev[0].elapsed_time(ev[1]))
+                ta.append(ev[1].elapsed_time(ev[2]))
+        ef = chk.rel(kg[0], ref_fwd)
+        ea = chk.rel(out[0], chk.adjoint(kg[0]))
+        fm, am = float(np.median(tf)), float(np.median(ta))
+        res[mode] = {"kernels": list(bp.kernel_names()), "fwd_ms": fm, "adj_ms": am,
+                     "value": N * C * B / ((fm + am) / 1e3), "rel_err_fwd_vs_fp64": ef, "rel_err_adj_vs_fp64": ea}
+        del kg, out
+    g.gridder_mode = saved
+    g._brick_plans = None
+    return res
+
+
 def cpu_baseline(coords, acr, spokes: int):
     """Reference CPU implementation timed on a bounded sample of the trajectory."""
     from oracle.ref_cpu import ReferenceCPU
@@ -383,7 +468,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--table-mode", default=None, choices=["tc", "tc1", "v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"])
+    ap.add_argument("--table-mode", default="tc",
+                    choices=["auto", "tc", "tc1", "v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"],
+                    help="gridder: tc = tensor-core bf16x3 (default), tc1 = bf16, v8 = FP32 CUDA cores, auto")
+    ap.add_argument("--no-precision-modes", action="store_true", help="skip the FP32 / bf16 comparison")
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
@@ -412,7 +500,7 @@ def main():
     torch.cuda.set_device(dev)
 
     g, coords, acr, data = build_workload(dev)
-    if args.table_mode:
+    if args.table_mode and args.table_mode != "auto":
         g.gridder_mode = args.table_mode
     bp = g._brick(0)
     G = int(np.prod(g.plan.grid_shape))
@@ -496,6 +584,22 @@ def main():
             "api": "GrogInterpolator.grid(pinned host tensor) + GrogInterpolator.degrid(host tensor)",
         }
 
+    # relative L2 error of the measured path against an FP64 restatement, and
+    # the FP32 CUDA-core / plain bf16 gridders on the same data
+    chk = Fp64Check(g, N, C)
+    ref_fwd = chk.forward(data[0])
+    accuracy = {"rel_err_fwd_vs_fp64": chk.rel(kgrid[0], ref_fwd),
+                "rel_err_adj_vs_fp64": chk.rel(out[0], chk.adjoint(kgrid[0])),
+                "tolerance": 1e-4}
+    modes = None
+    if ws == 1 and not args.no_precision_modes:
+        try:
+            modes = time_modes(g, data, [m for m in ("v8", "tc", "tc1") if m != "auto"], ref_fwd, chk)
+        except Exception as exc:  # noqa: BLE001
+            modes = {"error": f"{type(exc).__name__}: {exc}"}
+    del ref_fwd, chk
+    torch.cuda.empty_cache()
+
     serving = cg2 = c3 = None
     if ws == 1 and args.serve_seconds > 0 and not resized:
         try:
@@ -528,8 +632,10 @@ def main():
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "c64",
+            "dtype": {"tc": "bf16x3 (fp32 accumulate)", "tc1": "bf16 (fp32 accumulate)"}.get(bp.mode, "fp32"),
             "data": "synthetic",
+            "accuracy": accuracy,
+            "precision_modes": modes,
             "config": {
                 "workload": (f"grog3d_kooshball_{GRID_N}c12_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
                              else "grog3d_kooshball_192c12_fwd_adj"),

@@ -689,7 +689,8 @@ class GrogGridder:
         self.fwd6 = None
         self.pairs = False
         dev = target_idx.device
-        kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True)
+        kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True,
+                   full_subs=True)
         self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_rows=True, **kwt)
         first = _first_valid_mask(target_idx, kw)
         self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwt)

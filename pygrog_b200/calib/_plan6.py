@@ -75,6 +75,7 @@ class BrickPlan6:
         pair_lanes: bool = False,
         sample_order: bool = False,
         cell_rows: bool = False,
+        full_subs: bool = False,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -128,8 +129,13 @@ class BrickPlan6:
         pos = torch.arange(n, device=dev) - start[brick_id]
         nsub_b = (cnt + self.sub_cap - 1) // self.sub_cap
         sub_first = torch.cumsum(nsub_b, 0) - nsub_b
-        # near-equal sub-chunks inside a brick keep consecutive sub-chunks balanced
-        sub_id = sub_first[brick_id] + (pos * nsub_b[brick_id]) // torch.clamp(cnt[brick_id], min=1)
+        if full_subs:
+            # full sub-chunks first (every warp of the tensor-core kernels gets
+            # the same number of m-tiles), the remainder last
+            sub_id = sub_first[brick_id] + pos // self.sub_cap
+        else:
+            # near-equal sub-chunks inside a brick keep consecutive sub-chunks balanced
+            sub_id = sub_first[brick_id] + (pos * nsub_b[brick_id]) // torch.clamp(cnt[brick_id], min=1)
         n_subs = int(nsub_b.sum())
         # staging slots: distinct samples of a sub-chunk, ascending
         uk, inv = torch.unique_consecutive(sub_id * n_src + src, return_inverse=True)

@@ -62,8 +62,7 @@ struct Shape {
 
 template <int CP, int NS>
 struct Regs {
-  static constexpr int W = (NS + 1) * 2 * Shape<CP>::NFR;
-  static constexpr int MINB = W <= 80 ? 2 : 1;  // CTAs per SM the register budget allows
+  static constexpr int MINB = CP <= 12 ? 2 : 1;  // CTAs per SM the register budget (two m-tiles per warp) allows
 };
 
 struct Geom {
@@ -131,70 +130,101 @@ __device__ __forceinline__ void split2(float2 v, uint32_t& hi, uint32_t& lo) {
   lo = bf2_bits(__floats2bfloat162_rn(v.x - hf.x, v.y - hf.y));
 }
 
-// v[r][m] = complex coil 4 m + t of row g + 8 r of the lane's m-tile (g = lane / 4,
-// t = lane % 4).  One dense stage: v <- v W^T over the 16 rows, W's fragments
-// bh (heads) / bl (tails).
+// v[T][r][m] = complex coil 4 m + t of row g + 8 r of the lane's m-tile T
+// (g = lane / 4, t = lane % 4); a warp runs its two m-tiles side by side (two
+// independent instruction streams).  One dense stage: v <- v W^T over the 16
+// rows of each tile.  W's fragments come from shared memory, per n-tile one
+// 16-byte word group of heads and one of tails per lane (lane-contiguous:
+// conflict-free).
 template <int CP, int TERMS>
-__device__ __forceinline__ void mm_stage(float2 (&v)[2][Shape<CP>::NT], const uint32_t (&bh)[Shape<CP>::NFR],
-                                         const uint32_t (&bl)[Shape<CP>::NFR]) {
+__device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const uint4* __restrict__ wst, int lane) {
   constexpr int NT = Shape<CP>::NT, K16 = Shape<CP>::K16, K8 = Shape<CP>::K8;
-  uint32_t ah[2][NT], al[2][NT];
+  uint32_t ah[2][2][NT], al[2][2][NT];
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
+  for (int T = 0; T < 2; ++T)
 #pragma unroll
-    for (int m = 0; m < NT; ++m) {
-      if constexpr (TERMS == 3) {
-        split2(v[r][m], ah[r][m], al[r][m]);
-      } else {
-        ah[r][m] = bf2_bits(__floats2bfloat162_rn(v[r][m].x, v[r][m].y));
-        al[r][m] = 0u;
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int m = 0; m < NT; ++m) {
+        if constexpr (TERMS == 3) {
+          split2(v[T][r][m], ah[T][r][m], al[T][r][m]);
+        } else {
+          ah[T][r][m] = bf2_bits(__floats2bfloat162_rn(v[T][r][m].x, v[T][r][m].y));
+          al[T][r][m] = 0u;
+        }
       }
-    }
-  }
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) {
-    // products alternate between two accumulators (tails first): two short
-    // dependency chains instead of one long one
-    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-    int f = nt * (2 * K16 + K8);
+    const uint4 bh4 = wst[(nt * 2) * 32 + lane];
+    const uint4 bl4 = wst[(nt * 2 + 1) * 32 + lane];
+    const uint32_t bh[4] = {bh4.x, bh4.y, bh4.z, bh4.w};
+    const uint32_t bl[4] = {bl4.x, bl4.y, bl4.z, bl4.w};
+    // products alternate between two accumulators per tile (tails first)
+    float d[2][2][4];
+#pragma unroll
+    for (int T = 0; T < 2; ++T)
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) d[T][a][e] = 0.f;
     int q = 0;
 #pragma unroll
     for (int kc = 0; kc < K16; ++kc) {
+      const int f = 2 * kc;
       if constexpr (TERMS == 3) {
-        mma16(d[q & 1], al[0][2 * kc], al[1][2 * kc], al[0][2 * kc + 1], al[1][2 * kc + 1], bh[f], bh[f + 1]);
+#pragma unroll
+        for (int T = 0; T < 2; ++T)
+          mma16(d[T][q & 1], al[T][0][2 * kc], al[T][1][2 * kc], al[T][0][2 * kc + 1], al[T][1][2 * kc + 1], bh[f],
+                bh[f + 1]);
         ++q;
-        mma16(d[q & 1], ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bl[f], bl[f + 1]);
+#pragma unroll
+        for (int T = 0; T < 2; ++T)
+          mma16(d[T][q & 1], ah[T][0][2 * kc], ah[T][1][2 * kc], ah[T][0][2 * kc + 1], ah[T][1][2 * kc + 1], bl[f],
+                bl[f + 1]);
         ++q;
       }
-      mma16(d[q & 1], ah[0][2 * kc], ah[1][2 * kc], ah[0][2 * kc + 1], ah[1][2 * kc + 1], bh[f], bh[f + 1]);
+#pragma unroll
+      for (int T = 0; T < 2; ++T)
+        mma16(d[T][q & 1], ah[T][0][2 * kc], ah[T][1][2 * kc], ah[T][0][2 * kc + 1], ah[T][1][2 * kc + 1], bh[f],
+              bh[f + 1]);
       ++q;
-      f += 2;
     }
     if constexpr (K8) {
+      const int f = 2 * K16;
       if constexpr (TERMS == 3) {
-        mma8(d[q & 1], al[0][NT - 1], al[1][NT - 1], bh[f]);
+#pragma unroll
+        for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], al[T][0][NT - 1], al[T][1][NT - 1], bh[f]);
         ++q;
-        mma8(d[q & 1], ah[0][NT - 1], ah[1][NT - 1], bl[f]);
+#pragma unroll
+        for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bl[f]);
         ++q;
       }
-      mma8(d[q & 1], ah[0][NT - 1], ah[1][NT - 1], bh[f]);
+#pragma unroll
+      for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bh[f]);
     }
-    v[0][nt] = make_float2(d[0][0] + d[1][0], d[0][1] + d[1][1]);
-    v[1][nt] = make_float2(d[0][2] + d[1][2], d[0][3] + d[1][3]);
+#pragma unroll
+    for (int T = 0; T < 2; ++T) {
+      v[T][0][nt] = make_float2(d[T][0][0] + d[T][1][0], d[T][0][1] + d[T][1][1]);
+      v[T][1][nt] = make_float2(d[T][0][2] + d[T][1][2], d[T][0][3] + d[T][1][3]);
+    }
   }
 }
 
-// W fragments of all NS + 1 stages, global layout (stage, head/tail, word, lane)
+// W fragments of all NS + 1 stages into shared memory, layout (stage, n-tile,
+// head/tail, lane, 4 words) from the global layout (stage, head/tail, word, lane).
 template <int CP, int NS>
-__device__ __forceinline__ void load_w(const uint32_t* __restrict__ wfrag, int lane,
-                                       uint32_t (&wb)[NS + 1][2][Shape<CP>::NFR]) {
-  constexpr int NFR = Shape<CP>::NFR;
-#pragma unroll
-  for (int s = 0; s <= NS; ++s)
-#pragma unroll
-    for (int b = 0; b < 2; ++b)
-#pragma unroll
-      for (int f = 0; f < NFR; ++f) wb[s][b][f] = __ldg(wfrag + ((s * 2 + b) * NFR + f) * 32 + lane);
+__device__ __forceinline__ void stage_w(uint32_t* __restrict__ wsm, const uint32_t* __restrict__ wfrag) {
+  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, FPN = NFR / NT;
+  constexpr int total = (NS + 1) * NT * 2 * 32 * 4;
+  for (int i = threadIdx.x; i < total; i += kT) {
+    const int w = i & 3;
+    const int lane = (i >> 2) & 31;
+    const int b = (i >> 7) & 1;
+    const int snt = i >> 8;  // stage * NT + nt
+    const int s = snt / NT;
+    const int nt = snt - s * NT;
+    wsm[i] = w < FPN ? __ldg(wfrag + ((s * 2 + b) * NFR + nt * FPN + w) * 32 + lane) : 0u;
+  }
 }
 
 // One replica row's decoded metadata.
@@ -230,23 +260,26 @@ __device__ __forceinline__ int diag_index(const Row& r, int s) {
   return a == 0 ? r.ix0 : (a == 1 ? r.ix1 : r.ix2);
 }
 
-// The whole chain on one m-tile: NS + 1 dense stages with the diagonal phases
-// of table dt (NS, nsteps, CP) between them.
+// The whole chain on a warp's two m-tiles: NS + 1 dense stages with the
+// diagonal phases of table dt (NS, nsteps, row stride dstride) between them.
 template <int CP, int NS, int TERMS, bool ADJ>
-__device__ __forceinline__ void chain(float2 (&v)[2][Shape<CP>::NT], const uint32_t (&wb)[NS + 1][2][Shape<CP>::NFR],
-                                      const float2* __restrict__ dt, int nsteps, int dstride, const Row (&rw)[2],
-                                      int t) {
+__device__ __forceinline__ void chain(float2 (&v)[2][2][Shape<CP>::NT], const uint4* __restrict__ wsm,
+                                      const float2* __restrict__ dt, int nsteps, int dstride,
+                                      const Row (&rw)[2][2], int lane) {
   constexpr int NT = Shape<CP>::NT;
+  const int t = lane & 3;
 #pragma unroll
   for (int s = 0; s <= NS; ++s) {
-    mm_stage<CP, TERMS>(v, wb[s][0], wb[s][1]);
+    mm_stage<CP, TERMS>(v, wsm + s * NT * 2 * 32, lane);
     if (s < NS) {
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[r], s)) * dstride + t;
+      for (int T = 0; T < 2; ++T)
 #pragma unroll
-        for (int m = 0; m < NT; ++m) v[r][m] = cmul(v[r][m], drow[4 * m]);
-      }
+        for (int r = 0; r < 2; ++r) {
+          const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[T][r], s)) * dstride + t;
+#pragma unroll
+          for (int m = 0; m < NT; ++m) v[T][r][m] = cmul(v[T][r][m], drow[4 * m]);
+        }
     }
   }
 }
@@ -316,12 +349,13 @@ struct Phases {
 
 // Shared-memory layout in float2 units: phase tables | tile(s) | staging (x or results)
 struct Smem {
-  int dt, tile, tile_sz, xs, xs_sz, ms, wsm, total;
+  int dt, wf, tile, tile_sz, xs, xs_sz, ms, wsm, total;
   __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward) {
     dt = 0;
     const Phases ph(CP, NS, nsteps);
-    tile = (ph.copies * ph.copy_sz + 1) & ~1;
-    tile_sz = (cells * (CP + 1) + 1) & ~1;
+    wf = (ph.copies * ph.copy_sz + 1) & ~1;       // W fragments: (NS + 1) * (CP / 4) * 2 * 32 uint4
+    tile = wf + (NS + 1) * (CP / 4) * 2 * 32 * 2;  // float2 units
+    tile_sz = (cells * (forward ? CP + 1 : CP) + 1) & ~1;  // forward: odd stride, conflict-free flush
     xs = tile + (forward ? 1 : 2) * tile_sz;
     xs_sz = CP * (cap + 4);
     ms = xs + (forward ? 2 : 1) * xs_sz;  // 2 x cap replica metadata (int2)
@@ -446,7 +480,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
     const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
   extern __shared__ float4 smem4[];
-  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, TS = Shape<CP>::TS;
+  constexpr int NT = Shape<CP>::NT, TS = Shape<CP>::TS;
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;  // block-uniform
   const int cells = geom.bz * geom.by * geom.bx;
@@ -485,8 +519,8 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
   stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
   int u1 = ld_u(st.d1, st.p + 1 < p1);  // staging slots of the next sub-chunk, one iteration ahead
-  uint32_t wb[NS + 1][2][NFR];
-  load_w<CP, NS>(wfrag, lane, wb);
+  uint4* wsm = reinterpret_cast<uint4*>(base + lay.wf);
+  stage_w<CP, NS>(reinterpret_cast<uint32_t*>(wsm), wfrag);
   stage_phases(dt, dtab, CP, NS, nsteps, ph);
   for (int i = tid; i < lay.tile_sz; i += kT) tile[i] = make_float2(0.f, 0.f);
 
@@ -508,30 +542,33 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       const float2* xs = xs0 + buf * lay.xs_sz;
       const int2* msb = ms0 + buf * cap;
       const float* wsb = ws0 + buf * cap;
+      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp and warp + 8
+        Row rw[2][2];
+        float2 v[2][2][NT];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int mt = warp + 8 * j;
-        if (mt * 16 >= nr) break;  // warp-uniform
-        Row rw[2];
-        float2 v[2][NT];
+        for (int T = 0; T < 2; ++T)
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const int e = mt * 16 + 2 * g + r;  // cell-ordered rows: entry 2 g + r on row g + 8 r
-          const bool in = e < nr;
-          rw[r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
+          for (int r = 0; r < 2; ++r) {
+            const int e = (warp + 8 * T) * 16 + 2 * g + r;  // cell-ordered rows: entry 2 g + r on row g + 8 r
+            const bool in = e < nr;
+            rw[T][r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
 #pragma unroll
-          for (int m = 0; m < NT; ++m) {
-            const int c = 4 * m + t;
-            v[r][m] = (rw[r].on && (FULLC || c < C)) ? xs[c * XS + rw[r].slot] : make_float2(0.f, 0.f);
+            for (int m = 0; m < NT; ++m) {
+              const int c = 4 * m + t;
+              v[T][r][m] = (rw[T][r].on && (FULLC || c < C)) ? xs[c * XS + rw[T][r].slot] : make_float2(0.f, 0.f);
+            }
           }
+        chain<CP, NS, TERMS, false>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
+#pragma unroll
+        for (int T = 0; T < 2; ++T) {
+          if ((warp + 8 * T) * 16 >= nr) break;  // warp-uniform
+#pragma unroll
+          for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int m = 0; m < NT; ++m) v[T][r][m] = cscale(v[T][r][m], rw[T][r].w);
+          reduce_rows_to_tile<CP, FULLC>(v[T], rw[T], C, tile, g, t);
+          __syncwarp();
         }
-        chain<CP, NS, TERMS, false>(v, wb, dtl, nsteps, ph.stride, rw, t);
-#pragma unroll
-        for (int r = 0; r < 2; ++r)
-#pragma unroll
-          for (int m = 0; m < NT; ++m) v[r][m] = cscale(v[r][m], rw[r].w);
-        reduce_rows_to_tile<CP, FULLC>(v, rw, C, tile, g, t);
-        __syncwarp();
       }
     }
     __syncthreads();  // tile complete for this sub-chunk; staging buffer `buf` free
@@ -577,7 +614,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
     const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
   extern __shared__ float4 smem4[];
-  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, TS = Shape<CP>::TS;
+  constexpr int NT = Shape<CP>::NT, TS = CP;  // tiles filled by cp.async: plain stride
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;
   const int cells = geom.bz * geom.by * geom.bx;
@@ -618,8 +655,8 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
   issue_tile(st.i0.x, tiles);
   stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
-  uint32_t wb[NS + 1][2][NFR];
-  load_w<CP, NS>(wfrag, lane, wb);
+  uint4* wsm = reinterpret_cast<uint4*>(base + lay.wf);
+  stage_w<CP, NS>(reinterpret_cast<uint32_t*>(wsm), wfrag);
   stage_phases(dt, dtab, CP, NS, nsteps, ph);
   for (int i = tid; i < lay.xs_sz; i += kT) res[i] = make_float2(0.f, 0.f);
   int u0 = ld_u(st.d0, true);
@@ -642,41 +679,43 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
       const float2* tl = tiles + par * lay.tile_sz;
       const int2* msb = ms0 + mb * cap;
       const float* wsb = ws0 + mb * cap;
+      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp and warp + 8
+        Row rw[2][2];
+        float2 v[2][2][NT];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int mt = warp + 8 * j;
-        if (mt * 16 >= nr) break;  // warp-uniform
-        Row rw[2];
-        float2 v[2][NT];
+        for (int T = 0; T < 2; ++T)
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const int e = mt * 16 + 8 * r + g;  // sample-ordered rows: entry 8 r + g on row g + 8 r
-          const bool in = e < nr;
-          rw[r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
+          for (int r = 0; r < 2; ++r) {
+            const int e = (warp + 8 * T) * 16 + 8 * r + g;  // sample-ordered rows: entry 8 r + g on row g + 8 r
+            const bool in = e < nr;
+            rw[T][r] = decode<NS>(in ? msb[e] : make_int2(-1, 0), in ? wsb[e] : 0.f, in, cells, nu, nsteps);
 #pragma unroll
-          for (int m = 0; m < NT; ++m) {
-            const int c = 4 * m + t;
-            v[r][m] = (rw[r].on && (FULLC || c < C)) ? tl[rw[r].cell * TS + c] : make_float2(0.f, 0.f);
+            for (int m = 0; m < NT; ++m) {
+              const int c = 4 * m + t;
+              v[T][r][m] = (rw[T][r].on && (FULLC || c < C)) ? tl[rw[T][r].cell * TS + c] : make_float2(0.f, 0.f);
+            }
           }
-        }
-        chain<CP, NS, TERMS, true>(v, wb, dtl, nsteps, ph.stride, rw, t);
+        chain<CP, NS, TERMS, true>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          if (!rw[r].on) continue;
+        for (int T = 0; T < 2; ++T)
 #pragma unroll
-          for (int m = 0; m < NT; ++m) {
-            const int c = 4 * m + t;
-            if (FULLC || c < C) {
-              float2* dst = res + c * XS + rw[r].slot;
-              if (ACC) {
-                atomicAdd(&dst->x, rw[r].w * v[r][m].x);
-                atomicAdd(&dst->y, rw[r].w * v[r][m].y);
-              } else {
-                *dst = make_float2(rw[r].w * v[r][m].x, rw[r].w * v[r][m].y);
+          for (int r = 0; r < 2; ++r) {
+            if (!rw[T][r].on) continue;
+#pragma unroll
+            for (int m = 0; m < NT; ++m) {
+              const int c = 4 * m + t;
+              if (FULLC || c < C) {
+                float2* dst = res + c * XS + rw[T][r].slot;
+                const float2 y = cscale(v[T][r][m], rw[T][r].w);
+                if (ACC) {
+                  atomicAdd(&dst->x, y.x);
+                  atomicAdd(&dst->y, y.y);
+                } else {
+                  *dst = y;
+                }
               }
             }
           }
-        }
       }
     }
     __syncthreads();  // results complete; this brick's tile no longer read
