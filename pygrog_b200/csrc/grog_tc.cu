@@ -49,7 +49,7 @@ namespace pgb {
 namespace tc {
 
 constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk
-constexpr int kLast = 2, kSplit = 4;
+constexpr int kFirst = 1, kLast = 2, kSplit = 4;
 
 template <int CP>
 struct Shape {
@@ -284,13 +284,15 @@ __device__ __forceinline__ void chain(float2 (&v)[2][2][Shape<CP>::NT], const ui
   }
 }
 
-// Minimal per-CTA stream of sub-chunk descriptors, two ahead.
+// Per-CTA stream of sub-chunk descriptors: d loaded four ahead, the
+// {brick, flags} words three ahead, so the L2 prefetch of sub-chunk p + 2
+// and the staging of p + 1 never wait on a descriptor load.
 struct Stream {
   const int4* sd;
   const int2* si;
   int p, p1;
-  int4 d0, d1, d2;
-  int2 i0, i1;
+  int4 d0, d1, d2, d3;
+  int2 i0, i1, i2;
   __device__ __forceinline__ int4 ld_d(int q) const { return q < p1 ? __ldg(sd + q) : make_int4(0, 0, 0, 0); }
   __device__ __forceinline__ int2 ld_i(int q) const { return q < p1 ? __ldg(si + q) : make_int2(0, 0); }
   __device__ __forceinline__ void init(const int4* sd_, const int2* si_, int p0_, int p1_) {
@@ -301,21 +303,40 @@ struct Stream {
     d0 = ld_d(p);
     d1 = ld_d(p + 1);
     d2 = ld_d(p + 2);
+    d3 = ld_d(p + 3);
     i0 = ld_i(p);
     i1 = ld_i(p + 1);
+    i2 = ld_i(p + 2);
   }
   __device__ __forceinline__ void advance() {
     ++p;
     d0 = d1;
     d1 = d2;
+    d2 = d3;
     i0 = i1;
-    d2 = ld_d(p + 2);
-    i1 = ld_i(p + 1);
+    i1 = i2;
+    d3 = ld_d(p + 3);
+    i2 = ld_i(p + 2);
   }
 };
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2::evict_last [%0];\n" ::"l"(p));
+}
+
 __device__ __forceinline__ int n_slots(int4 d, int cap) { return min(max(d.w - d.z, 0), cap); }
 __device__ __forceinline__ int n_reps(int4 d, int cap) { return min(max(d.y - d.x, 0), cap); }
+
+// Prefetch the replica metadata and weights of sub-chunk d into L2.
+__device__ __forceinline__ void prefetch_meta(const int2* __restrict__ meta, const float* __restrict__ wts, int4 d,
+                                              int cap) {
+  const int nr = n_reps(d, cap);
+  const int i = threadIdx.x * 16;  // one 128-byte line of int2 per 16 entries
+  if (i < nr) {
+    prefetch_l2(meta + d.x + i);
+    if ((i & 31) == 0) prefetch_l2(wts + d.x + i);
+  }
+}
 
 // Stage the replica metadata and weights of sub-chunk d (cp.async).
 __device__ __forceinline__ void stage_meta(const int2* __restrict__ meta, const float* __restrict__ wts, int4 d,
@@ -513,12 +534,24 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     }
   };
 
+  auto prefetch_x = [&](int4 d, int u) {  // samples' coils of sub-chunk d into L2
+    if (tid < n_slots(d, cap) && u >= 0 && u < N) {
+      const float2* src = dat + u;
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (FULLC || c < C) prefetch_l2(src + static_cast<int64_t>(c) * N);
+    }
+  };
+
   Stream st;
   st.init(sd, si, p0, p1);
   stage_x(st.d0, ld_u(st.d0, true), xs0);
   stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
-  int u1 = ld_u(st.d1, st.p + 1 < p1);  // staging slots of the next sub-chunk, one iteration ahead
+  // staging slots of sub-chunks p + 1 (staged this iteration) and p + 2
+  // (prefetched into L2 this iteration), loaded two and one iterations ahead
+  int u1 = ld_u(st.d1, st.p + 1 < p1);
+  int u2 = ld_u(st.d2, st.p + 2 < p1);
   uint4* wsm = reinterpret_cast<uint4*>(base + lay.wf);
   stage_w<CP, NS>(reinterpret_cast<uint32_t*>(wsm), wfrag);
   stage_phases(dt, dtab, CP, NS, nsteps, ph);
@@ -531,11 +564,15 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       stage_x(st.d1, u1, xs0 + (buf ^ 1) * lay.xs_sz);
       stage_meta(meta, wts, st.d1, cap, ms0 + (buf ^ 1) * cap, ws0 + (buf ^ 1) * cap);
       commit();
+      if (st.p + 2 < p1) {
+        prefetch_x(st.d2, u2);
+        prefetch_meta(meta, wts, st.d2, cap);
+      }
       wait_groups<1>();
     } else {
       wait_groups<0>();
     }
-    const int u2 = ld_u(st.d2, st.p + 2 < p1);
+    const int u3 = ld_u(st.d3, st.p + 3 < p1);
     __syncthreads();  // staging buffer `buf` complete; tile zeroed / flushed
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
@@ -603,6 +640,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     if (!more) break;
     st.advance();
     u1 = u2;
+    u2 = u3;
     buf ^= 1;
   }
 }
@@ -648,6 +686,19 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
   auto ld_u = [&](int4 d, bool valid) -> int {
     return (valid && tid < n_slots(d, cap)) ? __ldg(uniq + d.z + tid) : -1;
   };
+  auto prefetch_tile = [&](int brick) {  // brick tile into L2
+    int z0, y0, x0;
+    origin(geom, brick, z0, y0, x0);
+    for (int cl = tid; cl < cells; cl += kT) {
+      int64_t flat;
+      if (!flat_of(geom, z0, y0, x0, cl, flat)) continue;
+      if ((cl & (geom.bx - 1)) != 0 && ((flat & 15) != 0)) continue;  // one prefetch per 128-byte line
+      const float2* src = grd + flat;
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (FULLC || c < C) prefetch_l2(src + static_cast<int64_t>(c) * G);
+    }
+  };
 
   Stream st;
   st.init(sd, si, p0, p1);
@@ -668,6 +719,10 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
       if (last) issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz);
       stage_meta(meta, wts, st.d1, cap, ms0 + (mb ^ 1) * cap, ws0 + (mb ^ 1) * cap);
       commit();
+      if (st.p + 2 < p1) {  // sub-chunk p + 2 into L2: its metadata and, if it starts an item, its tile
+        if (st.i2.y & kFirst) prefetch_tile(st.i2.x);
+        prefetch_meta(meta, wts, st.d2, cap);
+      }
       wait_groups<1>();
     } else {
       wait_groups<0>();
