@@ -362,6 +362,18 @@ PGB_API int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N
                                const void* dtab_h, int64_t nsteps, int64_t ndim, int64_t C, int64_t B,
                                int64_t terms, const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);
+/* Brick tiles of the tensor-core gridder move by tensor-memory-accelerator
+ * copies (one bulk tensor load / store / reduce-add per brick, mbarrier
+ * completion) when the grid allows it (even gx and brick width, 16-byte
+ * aligned grid, C a multiple of 4); otherwise by per-element async copies.
+ * pgb_grog_tc_use_tma(0 / 1) turns the tensor copies off / on for later calls
+ * (negative: query only) and returns the previous setting.  No reference
+ * counterpart (performance switch). */
+PGB_API int pgb_grog_tc_use_tma(int64_t enable);
+/* Number of tile waits that gave up (bounded mbarrier spin; the kernel then
+ * returns without writing that brick's results); reset when reset != 0.
+ * Synchronous.  No reference counterpart (diagnostics). */
+PGB_API int pgb_grog_tc_timeouts(int64_t* count, int64_t reset);
 
 /* Replica expansion of interpolate() (calib/_grog.py:668-695):
  * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]

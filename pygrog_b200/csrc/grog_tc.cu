@@ -41,7 +41,11 @@
 //             adjoint chain W3^H conj(Dx) W2^H conj(Dy) W1^H conj(Dz) W0^H per
 //             replica, w * y into a per-slot result buffer, flushed per
 //             sub-chunk (atomic adds for the secondary replicas)
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
 
 #include "common.cuh"
 
@@ -95,6 +99,10 @@ __device__ __forceinline__ void cp8(void* smem_dst, const void* gsrc, int bytes)
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void cp16_cg(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp4(void* smem_dst, const void* gsrc) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
@@ -104,6 +112,70 @@ template <int N>
 __device__ __forceinline__ void wait_groups() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+
+// ---- TMA brick tiles ---------------------------------------------------------
+// The grid (B, C, gz, gy, gx) complex64 is described to the tensor memory
+// accelerator as a float32 tensor of dims {2 gx, gy, gz, B C}; one box
+// {2 bx, by, bz, C} is one brick of all coils, laid out in shared memory as
+// [coil][cell] (cell = (z by + y) bx + x).  Loads complete on an mbarrier,
+// stores / reduce-adds are bulk groups.  No multicast.
+__device__ int g_tc_timeouts;  // mbarrier waits that gave up (see pgb_grog_tc_timeouts)
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase `parity` of `bar`; false (and a recorded
+// timeout) if it did not complete within the spin limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (threadIdx.x == 0) atomicAdd(&g_tc_timeouts, 1);
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_load_tile(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_tile(const CUtensorMap* map, int x, int y, int z, int w, const void* src,
+                                               bool add) {
+  if (add) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.4d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];\n" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(src))
+        : "memory");
+  } else {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(src))
+                 : "memory");
+  }
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
 // d += A B, A 16x16 (4 bf16x2 words), B 16x8 (2 words), fp32 accumulate
 __device__ __forceinline__ void mma16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
@@ -370,18 +442,24 @@ struct Phases {
 
 // Shared-memory layout in float2 units: phase tables | tile(s) | staging (x or results)
 struct Smem {
-  int dt, wf, tile, tile_sz, xs, xs_sz, ms, wsm, total;
-  __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward) {
+  int dt, wf, tile, tile_sz, xs, xs_sz, ms, wsm, bar, total;
+  __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward, bool tma = false) {
     dt = 0;
     const Phases ph(CP, NS, nsteps);
     wf = (ph.copies * ph.copy_sz + 1) & ~1;       // W fragments: (NS + 1) * (CP / 4) * 2 * 32 uint4
     tile = wf + (NS + 1) * (CP / 4) * 2 * 32 * 2;  // float2 units
-    tile_sz = (cells * (forward ? CP + 1 : CP) + 1) & ~1;  // forward: odd stride, conflict-free flush
+    if (tma) {
+      tile = (tile + 15) & ~15;  // 128-byte aligned TMA boxes, [coil][cell]
+      tile_sz = (cells * CP + 15) & ~15;
+    } else {
+      tile_sz = (cells * (forward ? CP + 1 : CP) + 1) & ~1;  // forward: odd stride, conflict-free flush
+    }
     xs = tile + (forward ? 1 : 2) * tile_sz;
     xs_sz = CP * (cap + 4);
     ms = xs + (forward ? 2 : 1) * xs_sz;  // 2 x cap replica metadata (int2)
     wsm = ms + 2 * cap;                   // 2 x cap replica weights (float)
-    total = wsm + cap;
+    bar = wsm + cap;                      // 2 mbarriers (uint64)
+    total = bar + 2;
   }
 };
 
@@ -405,9 +483,9 @@ __device__ __forceinline__ void stage_phases(float2* __restrict__ dt, const floa
 // and the last position of every run adds the total to tile[cell].  Runs
 // that do not cross the m-tile (straddle bit clear) have no other writer in
 // the sub-chunk and use plain read-modify-writes; the others add atomically.
-template <int CP, bool FULLC>
+template <int CP, bool FULLC, bool TMA>
 __device__ __forceinline__ void reduce_rows_to_tile(float2 (&v)[2][Shape<CP>::NT], const Row (&rw)[2], int C,
-                                                    float2* __restrict__ tile, int g, int t) {
+                                                    float2* __restrict__ tile, int cells, int g, int t) {
   constexpr int NT = Shape<CP>::NT, TS = Shape<CP>::TS;
   constexpr unsigned FULL = 0xffffffffu;
   const int k0 = rw[0].on ? rw[0].cell : -1 - 2 * g;  // invalid rows: unique keys, never written
@@ -421,16 +499,16 @@ __device__ __forceinline__ void reduce_rows_to_tile(float2 (&v)[2][Shape<CP>::NT
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       if (!rw[r].on) continue;
-      float2* dst = tile + rw[r].cell * TS;
+      float2* dst = tile + (TMA ? rw[r].cell : rw[r].cell * TS);
 #pragma unroll
       for (int m = 0; m < NT; ++m) {
         const int c = 4 * m + t;
         if (!FULLC && c >= C) continue;
         if (rw[r].straddle) {
-          atomicAdd(&dst[c].x, v[r][m].x);
-          atomicAdd(&dst[c].y, v[r][m].y);
+          atomicAdd(&dst[TMA ? c * cells : c].x, v[r][m].x);
+          atomicAdd(&dst[TMA ? c * cells : c].y, v[r][m].y);
         } else {
-          dst[c] = cadd(dst[c], v[r][m]);
+          dst[TMA ? c * cells : c] = cadd(dst[TMA ? c * cells : c], v[r][m]);
         }
       }
     }
@@ -464,48 +542,49 @@ __device__ __forceinline__ void reduce_rows_to_tile(float2 (&v)[2][Shape<CP>::NT
   // position 2 g ends a run when 2 g + 1 holds another cell
   if (!pair && rw[0].on) {
     const bool carry = k0 == kprev;
-    float2* dst = tile + rw[0].cell * TS;
+    float2* dst = tile + (TMA ? rw[0].cell : rw[0].cell * TS);
 #pragma unroll
     for (int m = 0; m < NT; ++m) {
       const int c = 4 * m + t;
       if (!FULLC && c >= C) continue;
       const float2 val = carry ? cadd(v[0][m], aprev[m]) : v[0][m];
       if (rw[0].straddle) {
-        atomicAdd(&dst[c].x, val.x);
-        atomicAdd(&dst[c].y, val.y);
+        atomicAdd(&dst[TMA ? c * cells : c].x, val.x);
+        atomicAdd(&dst[TMA ? c * cells : c].y, val.y);
       } else {
-        dst[c] = cadd(dst[c], val);
+        dst[TMA ? c * cells : c] = cadd(dst[TMA ? c * cells : c], val);
       }
     }
   }
   if (k1 != knext && rw[1].on) {
-    float2* dst = tile + rw[1].cell * TS;
+    float2* dst = tile + (TMA ? rw[1].cell : rw[1].cell * TS);
 #pragma unroll
     for (int m = 0; m < NT; ++m) {
       const int c = 4 * m + t;
       if (!FULLC && c >= C) continue;
       if (rw[1].straddle) {
-        atomicAdd(&dst[c].x, a[m].x);
-        atomicAdd(&dst[c].y, a[m].y);
+        atomicAdd(&dst[TMA ? c * cells : c].x, a[m].x);
+        atomicAdd(&dst[TMA ? c * cells : c].y, a[m].y);
       } else {
-        dst[c] = cadd(dst[c], a[m]);
+        dst[TMA ? c * cells : c] = cadd(dst[TMA ? c * cells : c], a[m]);
       }
     }
   }
 }
 
-template <int CP, int NS, int TERMS, bool FULLC>
+template <int CP, int NS, int TERMS, bool FULLC, bool TMA>
 __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G, int C,
     const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
     const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
-    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
-  extern __shared__ float4 smem4[];
+    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom,
+    const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) float4 smem4[];
   constexpr int NT = Shape<CP>::NT, TS = Shape<CP>::TS;
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;  // block-uniform
   const int cells = geom.bz * geom.by * geom.bx;
-  const Smem lay(CP, NS, nsteps, cells, cap, true);
+  const Smem lay(CP, NS, nsteps, cells, cap, true, TMA);
   const Phases ph(CP, NS, nsteps);
   const int XS = cap + 4;
   float2* base = reinterpret_cast<float2*>(smem4);
@@ -523,14 +602,27 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
   auto ld_u = [&](int4 d, bool valid) -> int {
     return (valid && tid < n_slots(d, cap)) ? __ldg(uniq + d.z + tid) : -1;
   };
+  // 16-byte copies need 16-byte aligned coil planes (even N, aligned base)
+  const bool pairs_ok = (N & 1) == 0 && (XS & 1) == 0 && (reinterpret_cast<uintptr_t>(dat) & 15) == 0;
   auto stage_x = [&](int4 d, int u, float2* xs) {  // samples' coils of sub-chunk d, coil-major
     const int nu = n_slots(d, cap);
-    if (tid < nu) {
-      const bool ok = u >= 0 && u < N;
+    // an even slot whose sample is even and whose odd neighbour holds the
+    // next sample copies both with one 16-byte copy (L2 only); its neighbour
+    // then copies nothing
+    const int un = __shfl_down_sync(0xffffffffu, u, 1);
+    const bool ok = tid < nu && u >= 0 && u < N;
+    const bool lead = pairs_ok && ok && (tid & 1) == 0 && lane != 31 && tid + 1 < nu && un == u + 1 && (u & 1) == 0;
+    const bool led = __shfl_up_sync(0xffffffffu, lead ? 1 : 0, 1) != 0 && (tid & 1) == 1;
+    if (tid < nu && !led) {
       const float2* src = ok ? dat + u : dat;
 #pragma unroll
-      for (int c = 0; c < CP; ++c)
-        if (FULLC || c < C) cp8(xs + c * XS + tid, ok ? src + static_cast<int64_t>(c) * N : dat, ok ? 8 : 0);
+      for (int c = 0; c < CP; ++c) {
+        if (!(FULLC || c < C)) continue;
+        if (lead)
+          cp16_cg(xs + c * XS + tid, src + static_cast<int64_t>(c) * N);
+        else
+          cp8(xs + c * XS + tid, ok ? src + static_cast<int64_t>(c) * N : dat, ok ? 8 : 0);
+      }
     }
   };
 
@@ -603,13 +695,24 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
           for (int r = 0; r < 2; ++r)
 #pragma unroll
             for (int m = 0; m < NT; ++m) v[T][r][m] = cscale(v[T][r][m], rw[T][r].w);
-          reduce_rows_to_tile<CP, FULLC>(v[T], rw[T], C, tile, g, t);
+          reduce_rows_to_tile<CP, FULLC, TMA>(v[T], rw[T], C, tile, cells, g, t);
           __syncwarp();
         }
       }
     }
+    if (TMA) fence_proxy_async();  // this thread's tile writes -> visible to the tensor-copy store
     __syncthreads();  // tile complete for this sub-chunk; staging buffer `buf` free
-    if (st.i0.y & kLast) {
+    if (TMA && (st.i0.y & kLast)) {  // one tensor store (reduce-add for split bricks) per brick
+      if (tid == 0) {
+        int z0, y0, x0;
+        origin(geom, st.i0.x, z0, y0, x0);
+        tma_store_tile(&tmap, 2 * x0, y0, z0, b * C, tile, (st.i0.y & kSplit) != 0);
+        bulk_wait_read_all();  // the tile has been read out: it can be cleared
+      }
+      __syncthreads();
+      float4* t4 = reinterpret_cast<float4*>(tile);
+      for (int i = tid; i < (C * cells) / 2; i += kT) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else if (st.i0.y & kLast) {
       int z0, y0, x0;
       origin(geom, st.i0.x, z0, y0, x0);
       const bool split = (st.i0.y & kSplit) != 0;
@@ -643,20 +746,25 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     u2 = u3;
     buf ^= 1;
   }
+  if (TMA && tid == 0) bulk_wait_all();
 }
 
-template <int CP, int NS, int TERMS, bool ACC, bool FULLC>
+template <int CP, int NS, int TERMS, bool ACC, bool FULLC, bool TMA>
 __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     const float2* __restrict__ grid, int64_t G, float2* __restrict__ out, int64_t N, int C,
     const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
     const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
-    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom) {
-  extern __shared__ float4 smem4[];
+    const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom,
+    const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) float4 smem4[];
   constexpr int NT = Shape<CP>::NT, TS = CP;  // tiles filled by cp.async: plain stride
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;
   const int cells = geom.bz * geom.by * geom.bx;
-  const Smem lay(CP, NS, nsteps, cells, cap, false);
+  const Smem lay(CP, NS, nsteps, cells, cap, false, TMA);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<float2*>(smem4) + lay.bar);
+  unsigned phase = 0;  // bit k: parity of the next completion of bars[k]
+  __shared__ int s_ok;
   const int XS = cap + 4;
   float2* base = reinterpret_cast<float2*>(smem4);
   float2* dt = base + lay.dt;
@@ -671,9 +779,17 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
   const float2* dtl = dt + (ph.copies == 4 ? (g & 3) * ph.copy_sz : 0);  // this lane's phase copy
 
-  auto issue_tile = [&](int brick, float2* tl) {  // one cell per thread, all coils
+  auto issue_tile = [&](int brick, float2* tl, int k) {  // brick tile of all coils into buffer k
     int z0, y0, x0;
     origin(geom, brick, z0, y0, x0);
+    if (TMA) {  // one tensor copy, completion on bars[k]
+      if (tid == 0) {
+        fence_proxy_async();  // earlier reads of this buffer precede the copy
+        mbar_expect_tx(bars + k, static_cast<unsigned>(C * cells * 8));
+        tma_load_tile(tl, &tmap, 2 * x0, y0, z0, b * C, bars + k);
+      }
+      return;
+    }
     for (int cl = tid; cl < cells; cl += kT) {
       int64_t flat;
       const bool in = flat_of(geom, z0, y0, x0, cl, flat);
@@ -700,10 +816,18 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     }
   };
 
+  if (TMA) {
+    if (tid == 0) {
+      mbar_init(bars, 1);
+      mbar_init(bars + 1, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+  }
   Stream st;
   st.init(sd, si, p0, p1);
   int par = 0, mb = 0;
-  issue_tile(st.i0.x, tiles);
+  issue_tile(st.i0.x, tiles, 0);
   stage_meta(meta, wts, st.d0, cap, ms0, ws0);
   commit();
   uint4* wsm = reinterpret_cast<uint4*>(base + lay.wf);
@@ -716,7 +840,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     const bool more = st.p + 1 < p1;
     const bool last = (st.i0.y & kLast) != 0;
     if (more) {  // next sub-chunk's metadata (and next brick's tile) during this compute
-      if (last) issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz);
+      if (last) issue_tile(st.i1.x, tiles + (par ^ 1) * lay.tile_sz, par ^ 1);
       stage_meta(meta, wts, st.d1, cap, ms0 + (mb ^ 1) * cap, ws0 + (mb ^ 1) * cap);
       commit();
       if (st.p + 2 < p1) {  // sub-chunk p + 2 into L2: its metadata and, if it starts an item, its tile
@@ -728,7 +852,13 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
       wait_groups<0>();
     }
     const int u1 = ld_u(st.d1, more);
+    const bool wait_tile = TMA && (st.i0.y & kFirst);  // this item's tile: its tensor copy
+    if (wait_tile && tid == 0) s_ok = mbar_wait(bars + par, (phase >> par) & 1) ? 1 : 0;
     __syncthreads();  // tile of this brick complete; previous results flushed
+    if (wait_tile) {
+      if (!s_ok) return;  // block-uniform: the copy never completed (recorded in g_tc_timeouts)
+      phase ^= 1u << par;
+    }
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
       const float2* tl = tiles + par * lay.tile_sz;
@@ -747,7 +877,9 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
 #pragma unroll
             for (int m = 0; m < NT; ++m) {
               const int c = 4 * m + t;
-              v[T][r][m] = (rw[T][r].on && (FULLC || c < C)) ? tl[rw[T][r].cell * TS + c] : make_float2(0.f, 0.f);
+              v[T][r][m] = (rw[T][r].on && (FULLC || c < C))
+                               ? tl[TMA ? c * cells + rw[T][r].cell : rw[T][r].cell * TS + c]
+                               : make_float2(0.f, 0.f);
             }
           }
         chain<CP, NS, TERMS, true>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
@@ -872,6 +1004,50 @@ static int check_common(const char* who, int64_t C, int64_t N, int64_t B, int64_
 using namespace pgb;
 using namespace pgb::tc;
 
+namespace {
+
+bool g_use_tma = true;
+
+// Tensor map of the grid (B, C, gz, gy, gx) complex64 as float32 {2 gx, gy, gz, B C}
+// with one brick of all coils per box.  False when the layout cannot be
+// described (odd gx or brick width, unaligned base) or the driver entry point
+// is missing; the kernels then stage tiles with per-element copies.
+bool make_tile_map(CUtensorMap* map, const void* grid, const pgb_v6_plan* p, int64_t C, int64_t B) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static bool looked_up = false;
+  if (!g_use_tma) return false;
+  if (!looked_up) {
+    looked_up = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    else
+      cudaGetLastError();
+  }
+  if (encode == nullptr) return false;
+  if ((p->gx & 1) || (p->bx & 1) || (reinterpret_cast<uintptr_t>(grid) & 15) != 0) return false;
+  if (2 * p->bx > 256 || p->by > 256 || p->bz > 256 || C > 256 || B * C > (int64_t(1) << 31)) return false;
+  const cuuint64_t gx = p->gx, gy = p->gy, gz = p->gz;
+  cuuint64_t dims[4] = {2 * gx, gy, gz, static_cast<cuuint64_t>(B * C)};
+  cuuint64_t strides[3] = {gx * 8, gx * gy * 8, gx * gy * gz * 8};
+  cuuint32_t box[4] = {static_cast<cuuint32_t>(2 * p->bx), static_cast<cuuint32_t>(p->by),
+                       static_cast<cuuint32_t>(p->bz), static_cast<cuuint32_t>(C)};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(grid), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t tc_smem(int64_t C, int cells, int64_t nsteps, int64_t ndim, int cap, bool fwd, bool tma) {
+  return static_cast<size_t>(Smem(padded(C), static_cast<int>(ndim), static_cast<int>(nsteps), cells, cap, fwd, tma)
+                                 .total) *
+         sizeof(float2);
+}
+
+}  // namespace
+
 #define PGB_TC_DISPATCH(X) \
   X(4, 2) X(4, 3) X(8, 2) X(8, 3) X(12, 2) X(12, 3) X(16, 2) X(16, 3)
 
@@ -882,9 +1058,14 @@ size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t 
       sub_cap < 1 || sub_cap > kT)
     return ~static_cast<size_t>(0);
   const int CP = padded(C), NS = static_cast<int>(ndim);
-  const size_t a = Smem(CP, NS, static_cast<int>(nsteps), static_cast<int>(cells), static_cast<int>(sub_cap), true).total;
-  const size_t b = Smem(CP, NS, static_cast<int>(nsteps), static_cast<int>(cells), static_cast<int>(sub_cap), false).total;
-  return (a > b ? a : b) * sizeof(float2);
+  size_t m = 0;
+  for (int tma = 0; tma < 2; ++tma)
+    for (int fwd = 0; fwd < 2; ++fwd) {
+      const size_t v = Smem(CP, NS, static_cast<int>(nsteps), static_cast<int>(cells), static_cast<int>(sub_cap),
+                            fwd != 0, tma != 0).total;
+      m = v > m ? v : m;
+    }
+  return m * sizeof(float2);
 }
 
 int pgb_grog_tc_blocks_per_sm(int64_t C, int64_t ndim) {
@@ -929,20 +1110,26 @@ int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const v
   }
   if (plan->n_cta == 0) return PGB_OK;
   dim3 grd(plan->n_cta, static_cast<unsigned>(B));
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  const bool tma = C == padded(C) && make_tile_map(&tmap, grid, plan, C, B);
+  const size_t smem_k = tc_smem(C, cells, nsteps, ndim, plan->sub_cap, true, tma);
   const int key = padded(C) * 10 + static_cast<int>(ndim);
   switch (key) {
 #define X(CP, NS)                                                                                               \
   case CP * 10 + NS: {                                                                                          \
     const bool full = C == CP;                                                                                  \
-    auto k = terms == 3 ? (full ? grog_grid_tc_kernel<CP, NS, 3, true> : grog_grid_tc_kernel<CP, NS, 3, false>)    \
-                        : (full ? grog_grid_tc_kernel<CP, NS, 1, true> : grog_grid_tc_kernel<CP, NS, 1, false>);   \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
-    k<<<grd, kT, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,                 \
-                            static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \
-                            static_cast<const float2*>(dtab), static_cast<int>(nsteps),                         \
-                            reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),    \
-                            plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,       \
-                            plan->sub_cap, geom);                                                               \
+    auto k = terms == 3 ? (tma ? grog_grid_tc_kernel<CP, NS, 3, true, true>                                     \
+                               : (full ? grog_grid_tc_kernel<CP, NS, 3, true, false> : grog_grid_tc_kernel<CP, NS, 3, false, false>)) \
+                        : (tma ? grog_grid_tc_kernel<CP, NS, 1, true, true>                                     \
+                               : (full ? grog_grid_tc_kernel<CP, NS, 1, true, false> : grog_grid_tc_kernel<CP, NS, 1, false, false>)); \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_k);                          \
+    k<<<grd, kT, smem_k, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,               \
+                              static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                         \
+                              static_cast<const float2*>(dtab), static_cast<int>(nsteps),                       \
+                              reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),  \
+                              plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,     \
+                              plan->sub_cap, geom, tmap);                                                       \
   } break;
     PGB_TC_DISPATCH(X)
 #undef X
@@ -966,26 +1153,31 @@ int degrid_tc_one(const char* who, const void* grid, int64_t G, void* out, int64
   const size_t smem = pgb_grog_tc_smem_bytes(C, cells, nsteps, ndim, plan->sub_cap);
   PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED, "%s: tiles + results need %zu B of shared memory", who, smem);
   dim3 grd(plan->n_cta, static_cast<unsigned>(B));
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  const bool tma = C == padded(C) && make_tile_map(&tmap, grid, plan, C, B);
+  const size_t smem_k = tc_smem(C, cells, nsteps, ndim, plan->sub_cap, false, tma);
   const int key = padded(C) * 10 + static_cast<int>(ndim);
   switch (key) {
+#define PGB_TC_DEG(P, Q, T3, A)                                                                                 \
+  (tma ? grog_degrid_tc_kernel<P, Q, T3, A, true, true>                                                         \
+       : (full ? grog_degrid_tc_kernel<P, Q, T3, A, true, false> : grog_degrid_tc_kernel<P, Q, T3, A, false, false>))
 #define X(CP, NS)                                                                                               \
   case CP * 10 + NS: {                                                                                          \
     const bool full = C == CP;                                                                                  \
-    auto k = terms == 3                                                                                         \
-                 ? (acc ? (full ? grog_degrid_tc_kernel<CP, NS, 3, true, true> : grog_degrid_tc_kernel<CP, NS, 3, true, false>)     \
-                        : (full ? grog_degrid_tc_kernel<CP, NS, 3, false, true> : grog_degrid_tc_kernel<CP, NS, 3, false, false>))  \
-                 : (acc ? (full ? grog_degrid_tc_kernel<CP, NS, 1, true, true> : grog_degrid_tc_kernel<CP, NS, 1, true, false>)     \
-                        : (full ? grog_degrid_tc_kernel<CP, NS, 1, false, true> : grog_degrid_tc_kernel<CP, NS, 1, false, false>)); \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                            \
-    k<<<grd, kT, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                  \
-                            static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                           \
-                            static_cast<const float2*>(dtab), static_cast<int>(nsteps),                         \
-                            reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),    \
-                            plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,       \
-                            plan->sub_cap, geom);                                                               \
+    auto k = terms == 3 ? (acc ? PGB_TC_DEG(CP, NS, 3, true) : PGB_TC_DEG(CP, NS, 3, false))                    \
+                        : (acc ? PGB_TC_DEG(CP, NS, 1, true) : PGB_TC_DEG(CP, NS, 1, false));                   \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_k);                          \
+    k<<<grd, kT, smem_k, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                \
+                              static_cast<int>(C), static_cast<const uint32_t*>(wfrag),                         \
+                              static_cast<const float2*>(dtab), static_cast<int>(nsteps),                       \
+                              reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),  \
+                              plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,     \
+                              plan->sub_cap, geom, tmap);                                                       \
   } break;
     PGB_TC_DISPATCH(X)
 #undef X
+#undef PGB_TC_DEG
     default:
       PGB_REQUIRE(false, PGB_ERR_UNSUPPORTED, "%s: no kernel for C=%lld ndim=%lld", who, (long long)C,
                   (long long)ndim);
@@ -1035,6 +1227,31 @@ int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N, const 
     zero_samples_tc<<<grid_for(n_zero * C * B, 256), 256, 0, s>>>(static_cast<float2*>(out), N, static_cast<int>(C),
                                                                   static_cast<int>(B), zero_src, n_zero);
     PGB_LAUNCH_CHECK(who);
+  }
+  return PGB_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int pgb_grog_tc_use_tma(int64_t enable) {
+  const int prev = g_use_tma ? 1 : 0;
+  if (enable >= 0) g_use_tma = enable != 0;
+  return prev;
+}
+
+int pgb_grog_tc_timeouts(int64_t* count, int64_t reset) {
+  clear_error();
+  PGB_REQUIRE(count != nullptr, PGB_ERR_INVALID, "grog_tc_timeouts: null output");
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_timeouts, sizeof(int));
+  PGB_REQUIRE(e == cudaSuccess, PGB_ERR_CUDA, "grog_tc_timeouts: %s", cudaGetErrorString(e));
+  *count = v;
+  if (reset) {
+    const int z = 0;
+    e = cudaMemcpyToSymbol(g_tc_timeouts, &z, sizeof(int));
+    PGB_REQUIRE(e == cudaSuccess, PGB_ERR_CUDA, "grog_tc_timeouts: %s", cudaGetErrorString(e));
   }
   return PGB_OK;
 }
