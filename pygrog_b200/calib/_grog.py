@@ -493,6 +493,8 @@ class GrogGridder:
     # v8 forward: longest run of one cell's replicas summed by one thread
     SEG_LEN_V8 = 24
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
+    # tensor-core forward plans: cell runs packed into 16-row m-tiles (0: off)
+    PACK_ROWS_TC = 16
 
     def __init__(self, target_idx, interp_idx, rep_weight, kw, grid_shape, table, factors, nsteps,
                  mode: str | None = None, brick=None, chunk: int = 2048, tc_ops: dict | None = None):
@@ -691,7 +693,8 @@ class GrogGridder:
         dev = target_idx.device
         kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True,
                    full_subs=True)
-        self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_rows=True, **kwt)
+        self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_rows=True,
+                               pack_rows=self.PACK_ROWS_TC, **kwt)
         first = _first_valid_mask(target_idx, kw)
         self.adj_plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwt)
         self.plan2 = None

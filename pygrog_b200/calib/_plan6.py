@@ -76,6 +76,7 @@ class BrickPlan6:
         sample_order: bool = False,
         cell_rows: bool = False,
         full_subs: bool = False,
+        pack_rows: int = 0,
     ):
         dev = target_idx.device
         grid_shape = tuple(int(s) for s in grid_shape)
@@ -127,12 +128,17 @@ class BrickPlan6:
         cnt = torch.bincount(brick_id, minlength=n_bricks)
         start = torch.cumsum(cnt, 0) - cnt
         pos = torch.arange(n, device=dev) - start[brick_id]
-        nsub_b = (cnt + self.sub_cap - 1) // self.sub_cap
+        # with pack_rows, sub-chunks take sub_cap - pack_rows replicas and keep
+        # pack_rows entries for the padding that aligns cell runs to m-tiles
+        form_cap = self.sub_cap - pack_rows if (cell_rows and pack_rows) else self.sub_cap
+        if form_cap < 1:
+            raise ValueError("sub_cap must exceed pack_rows")
+        nsub_b = (cnt + form_cap - 1) // form_cap
         sub_first = torch.cumsum(nsub_b, 0) - nsub_b
         if full_subs:
             # full sub-chunks first (every warp of the tensor-core kernels gets
             # the same number of m-tiles), the remainder last
-            sub_id = sub_first[brick_id] + pos // self.sub_cap
+            sub_id = sub_first[brick_id] + pos // form_cap
         else:
             # near-equal sub-chunks inside a brick keep consecutive sub-chunks balanced
             sub_id = sub_first[brick_id] + (pos * nsub_b[brick_id]) // torch.clamp(cnt[brick_id], min=1)
@@ -201,10 +207,57 @@ class BrickPlan6:
             run_pos = pos[head]
             rs = run_pos[run_id]
             re = rs + run_len[run_id] - 1
-            straddle = (rs // 16) != (re // 16)
-            self.meta = torch.stack([cl | (slot << 16) | (straddle.to(torch.int64) << 30), q | (k << 16)],
-                                    dim=1).to(torch.int32).contiguous()
-            self.w = w.contiguous()
+            if pack_rows:
+                # next-fit of the runs into m-tiles of pack_rows rows: a run that
+                # would cross a boundary starts the next m-tile (padding entries,
+                # meta -1, in between) while the sub-chunk's padding budget
+                # allows; only runs longer than an m-tile still cross one
+                rsub = sub_id[head]
+                rk = torch.arange(run_len.numel(), device=dev) - (torch.cumsum(
+                    torch.bincount(rsub, minlength=n_subs), 0) - torch.bincount(rsub, minlength=n_subs))[rsub]
+                max_r = int(rk.max()) + 1
+                L2 = torch.zeros(n_subs, max_r, dtype=torch.int64, device=dev)
+                L2[rsub, rk] = run_len
+                rem = L2.flip(1).cumsum(1).flip(1)
+                cur = torch.zeros(n_subs, dtype=torch.int64, device=dev)
+                starts = torch.zeros_like(L2)
+                T = pack_rows
+                for kk in range(max_r):
+                    ln = L2[:, kk]
+                    off = cur % T
+                    pad = torch.where((ln > 0) & (ln <= T) & (off + ln > T), T - off, torch.zeros_like(off))
+                    pad = torch.where(cur + pad + rem[:, kk] <= self.sub_cap, pad, torch.zeros_like(pad))
+                    cur = cur + pad
+                    starts[:, kk] = cur
+                    cur = cur + ln
+                new_pos = starts[rsub, rk][run_id] + (pos - rs)
+                nslot = cur  # entries per sub-chunk, padding included
+                sbase = torch.cumsum(nslot, 0) - nslot
+                total = int(nslot.sum())
+                dest = sbase[sub_id] + new_pos
+                pad = torch.ones(total, dtype=torch.bool, device=dev)
+                pad[dest] = False
+                rs = starts[rsub, rk][run_id]
+                re = rs + run_len[run_id] - 1
+                straddle = (rs // T) != (re // T)
+
+                def spread(v, fill):
+                    out = torch.full((total,), fill, dtype=v.dtype, device=dev)
+                    out[dest] = v
+                    return out
+
+                meta0 = spread(cl | (slot << 16) | (straddle.to(torch.int64) << 30), -1)
+                meta1 = spread(q | (k << 16), 0)
+                self.meta = torch.stack([meta0, meta1], dim=1).to(torch.int32).contiguous()
+                self.w = spread(w, 0.0).contiguous()
+                src = spread(src, -1)
+                cl = spread(cl, cells)
+                sub_id = torch.searchsorted(sbase, torch.arange(total, device=dev), right=True) - 1
+            else:
+                straddle = (rs // 16) != (re // 16)
+                self.meta = torch.stack([cl | (slot << 16) | (straddle.to(torch.int64) << 30), q | (k << 16)],
+                                        dim=1).to(torch.int32).contiguous()
+                self.w = w.contiguous()
         elif sample_order:
             # keep step (1)'s sample order: the tensor-core gridder reads each
             # m-tile's staged samples in order (conflict-free) and spreads

@@ -363,3 +363,50 @@ def test_cell_row_plan_runs_and_straddle_bits():
     assert p.n_valid == q.n_valid == n_src
     assert sorted(zip(cell.tolist(), p.w.numpy().round(6).tolist())) == \
         sorted(zip((q.meta.numpy()[:, 0] & 0xFFFF).tolist(), q.w.numpy().round(6).tolist()))
+
+
+def test_cell_row_plan_packs_runs_into_m_tiles():
+    """With pack_rows, runs of at most 16 entries never cross a 16-entry
+    m-tile; padding entries (meta -1, weight 0) fill the gaps and every
+    replica appears once."""
+    import torch
+
+    from pygrog_b200.calib._plan6 import BrickPlan6
+
+    rng = np.random.default_rng(4)
+    n_src, kw, gs = 6000, 1, (16, 32, 32)
+    tgt = torch.as_tensor(rng.integers(0, 2500, (n_src, kw)))  # runs of 1-6 replicas per cell and sub-chunk
+    tgt[::97] = 123  # and one long run
+    idx = torch.as_tensor(rng.integers(0, 11 ** 3, (n_src, kw)))
+    w = torch.rand(n_src, kw) + 0.1
+    p = BrickPlan6(tgt, idx, w, kw, gs, brick=(4, 8, 8), n_outer=11, sub_cap=256, n_cta=4, sample_order=True,
+                   cell_rows=True, full_subs=True, pack_rows=16)
+    meta = p.meta.numpy()
+    valid = meta[:, 0] >= 0
+    assert valid.sum() == n_src and p.n_pad == (~valid).sum()
+    assert (p.w.numpy()[~valid] == 0).all()
+    crossing = 0
+    for b, e, _, _ in p.subs.numpy():
+        assert e - b <= 256
+        m = meta[b:e]
+        c = np.where(m[:, 0] >= 0, m[:, 0] & 0xFFFF, -1)
+        strad = (m[:, 0] >> 30) & 1
+        for v in np.unique(c[c >= 0]):
+            pos = np.nonzero(c == v)[0]
+            assert (np.diff(pos) == 1).all()  # one contiguous run
+            crosses = pos[0] // 16 != pos[-1] // 16
+            assert (strad[pos] == crosses).all()
+            if crosses and pos.size <= 16:
+                crossing += 1
+    # only runs that met an exhausted padding budget may still cross: far fewer
+    # than without packing
+    q0 = BrickPlan6(tgt, idx, w, kw, gs, brick=(4, 8, 8), n_outer=11, sub_cap=256, n_cta=4, sample_order=True,
+                    cell_rows=True, full_subs=True)
+    before = int(((q0.meta.numpy()[:, 0] >> 30) & 1).sum())
+    after = int(((meta[valid, 0] >> 30) & 1).sum())
+    assert crossing <= 0.25 * p.n_subs and after < 0.5 * before
+    q = BrickPlan6(tgt, idx, w, kw, gs, brick=(4, 8, 8), n_outer=11, sub_cap=256, n_cta=4, sample_order=True,
+                   cell_rows=True, full_subs=True)
+    qm = q.meta.numpy()
+    assert sorted(zip((meta[valid, 0] & 0xFFFF).tolist(), p.w.numpy()[valid].round(6).tolist())) == \
+        sorted(zip((qm[:, 0] & 0xFFFF).tolist(), q.w.numpy().round(6).tolist()))
