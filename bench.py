@@ -472,6 +472,8 @@ def main():
                     choices=["auto", "tc", "tc1", "v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"],
                     help="gridder: tc = tensor-core bf16x3 (default), tc1 = bf16, v8 = FP32 CUDA cores, auto")
     ap.add_argument("--no-precision-modes", action="store_true", help="skip the FP32 / bf16 comparison")
+    ap.add_argument("--autotune", action="store_true",
+                    help="report the gridder autotuner's trials (families x bricks) on this workload")
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
@@ -599,6 +601,16 @@ def main():
             modes = {"error": f"{type(exc).__name__}: {exc}"}
     del ref_fwd, chk
     torch.cuda.empty_cache()
+    tune = None
+    if args.autotune and ws == 1:
+        from pygrog_b200.calib import autotune_gridder
+
+        saved_mode = getattr(g, "gridder_mode", None)
+        tune = autotune_gridder(g, batch=B, tolerance=1e-4, reps=3)
+        tune["trials"] = [[m, list(b), t] for m, b, t in tune["trials"]]
+        tune["brick"] = list(tune["brick"])
+        g.gridder_mode, g.gridder_brick, g._brick_plans = saved_mode, None, None
+        torch.cuda.empty_cache()
 
     serving = cg2 = c3 = None
     if ws == 1 and args.serve_seconds > 0 and not resized:
@@ -636,6 +648,7 @@ def main():
             "data": "synthetic",
             "accuracy": accuracy,
             "precision_modes": modes,
+            "autotune": tune,
             "config": {
                 "workload": (f"grog3d_kooshball_{GRID_N}c12_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
                              else "grog3d_kooshball_192c12_fwd_adj"),

@@ -982,7 +982,7 @@ class GrogInterpolator:
             mode = getattr(self, "gridder_mode", None)
             tc_ops = self._tc_operands() if mode in ("tc", "tc1") else None
             bp = GrogGridder(tgt, idx, rep_w, kw, plan.grid_shape, self._interp_kernel, self._factors,
-                             self._nsteps, mode=mode, tc_ops=tc_ops)
+                             self._nsteps, mode=mode, tc_ops=tc_ops, brick=getattr(self, "gridder_brick", None))
             self._brick_plans[s] = bp
         return bp
 

@@ -192,3 +192,63 @@ def test_tensor_core_grid_degrid_vs_fp64_oracle(cuda, ndim, n, spokes, readout, 
     assert rel_l2(out.reshape(B, C, -1), ref_a) < tol
     # repeat: same result (the shared tile / result buffers are re-zeroed)
     assert rel_l2(g.grid(data), kg) < 1e-6
+
+
+def test_tensor_core_fallback_paths_match(cuda):
+    """Odd grid width (no tensor copies of brick tiles) and the tensor copies
+    switched off give the same operator as the default path."""
+    from pygrog_b200 import _lib
+
+    lib = _lib.load_library()
+    for n, osf in ((45, 1.0), (48, 1.0)):  # gx = 45: per-element tile copies; 48: tensor copies
+        coords, calib, data = _random_case(2, n, 24, 96, 8, osf, 2, "circle", 1, seed=n)
+        g = GrogInterpolator(shape=(n, n), coords=coords, oversamp=osf, kernel_width=2, device=cuda)
+        g.calc_interp_table(calib, lamda=0.01, precision=1)
+        g.gridder_mode = "tc"
+        table = g._interp_kernel.numpy().astype(np.complex128)
+        p = og.create_plan((n, n), coords, osf, 2, "circle")
+        qi = g._interp_idx.cpu().numpy()
+        ref, _ = og.grid(data.reshape(1, 8, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
+        kg = g.grid(data)
+        assert rel_l2(kg.reshape(1, 8, -1), ref) < 1e-4
+        prev = lib.pgb_grog_tc_use_tma(0)
+        try:
+            g._brick_plans = None
+            kg0 = g.grid(data)
+            back0 = g.degrid(kg)
+        finally:
+            lib.pgb_grog_tc_use_tma(prev)
+        g._brick_plans = None
+        back = g.degrid(kg)
+        assert rel_l2(kg0, kg) < 1e-6 and rel_l2(back0, back) < 1e-6
+    cnt = (__import__("ctypes").c_int64 * 1)()
+    _lib.call("pgb_grog_tc_timeouts", cnt, 0)
+    assert cnt[0] == 0
+
+
+def test_autotuner_picks_a_valid_gridder(cuda):
+    """The autotuner times the families that fit, installs the fastest, and
+    the installed gridder still matches the FP64 oracle within its family's
+    tolerance; a second call is served from the cache."""
+    from pygrog_b200.calib import autotune_gridder
+    from pygrog_b200.calib._autotune import clear_cache
+
+    clear_cache()
+    coords, calib, data = _random_case(3, 24, 300, 48, 12, 1.0, 2, "sphere", 1, seed=11)
+    g = GrogInterpolator(shape=(24,) * 3, coords=coords, oversamp=1.0, kernel_width=2, kernel_shape="sphere",
+                         device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    res = autotune_gridder(g, tolerance=1e-4, reps=2)
+    assert not res["cached"] and res["trials"] and res["mode"] in ("tc", "v8", "v6")
+    assert min(t[2] for t in res["trials"]) == res["ms"]
+    table = g._interp_kernel.numpy().astype(np.complex128)
+    p = og.create_plan((24,) * 3, coords, 1.0, 2, "sphere")
+    qi = g._interp_idx.cpu().numpy()
+    ref, _ = og.grid(data.reshape(1, 12, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
+    assert rel_l2(g.grid(data).reshape(1, 12, -1), ref) < 1e-4
+    again = autotune_gridder(g, tolerance=1e-4)
+    assert again["cached"] and again["mode"] == res["mode"] and again["brick"] == res["brick"]
+    # FP32 only: no tensor-core family among the candidates
+    clear_cache()
+    strict = autotune_gridder(g, tolerance=1e-6, reps=1)
+    assert all(t[0] in ("v8", "v6") for t in strict["trials"])
