@@ -128,6 +128,24 @@ def _profile_traffic(kernel: str):
     return None, None
 
 
+def aggregate_replicas(ms: float, units_per_rank: float, dist=None, device=None) -> tuple[float, float]:
+    """Whole-job numbers of N independent replicas: the step time is the
+    maximum over ranks and the throughput is the units of all ranks divided
+    by it (one process per GPU, no data-path collective; `dist` is
+    ``torch.distributed`` with an initialised group, or None for one rank)."""
+    if dist is None:
+        return ms, units_per_rank / (ms / 1e3)
+    import torch
+
+    t = torch.tensor([ms, units_per_rank], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    tot = t.clone()
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    max_ms = float(mx[0].item())
+    return max_ms, float(tot[1].item()) / (max_ms / 1e3)
+
+
 def build_workload(device, seed: int = 1001):
     """Plan + table + device-resident data for the 3-D configuration."""
     import torch
@@ -546,11 +564,7 @@ def main():
     fwd_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
     adj_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
     ms = total_ms / args.steps
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = ws * N * C * B / (ms / 1e3)
+    ms, value = aggregate_replicas(ms, float(N * C * B), dist, dev)
 
     # algorithmic bytes per launch (both directions): samples + per-replica metadata + grid
     alg_bytes = N * C * 8 * B + bp.n_valid * 12 + G * C * 8 * B
