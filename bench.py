@@ -281,6 +281,57 @@ def time_modes(g, data, modes, ref_fwd, chk, reps: int = 6, warm: int = 3) -> di
     return res
 
 
+def coil_compress_c1(dev, reps: int = 5) -> dict:
+    """The step before the path at the 3-D configuration: 32 raw coils of all
+    7.68 M samples compressed to 12 virtual coils (FP64 covariance of every
+    sample, host eigendecomposition, one HBM-bound compression pass)."""
+    import torch
+
+    from pygrog_b200 import _lib
+    from pygrog_b200.utils import compression_matrix
+
+    N = N_SPOKES * N_READOUT
+    gen = torch.Generator(device=dev).manual_seed(7)
+    raw = torch.randn(N_COILS_RAW, N, dtype=torch.complex64, device=dev, generator=gen)
+    out = torch.empty(N_COILS, N, dtype=torch.complex64, device=dev)
+    st = _lib.stream_ptr(dev)
+    t0 = time.perf_counter()
+    mat = compression_matrix(raw, N_COILS)
+    torch.cuda.synchronize(dev)
+    fit_s = time.perf_counter() - t0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ts = []
+    for it in range(reps + 2):
+        ev[0].record()
+        _lib.call("pgb_coil_compress", raw.data_ptr(), N, N_COILS_RAW, N_COILS, 1, mat.data_ptr(), out.data_ptr(), st)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        if it >= 2:
+            ts.append(ev[0].elapsed_time(ev[1]))
+    ms = float(np.median(ts))
+    ref = out.clone()
+    ts = []
+    for it in range(reps + 2):
+        ev[0].record()
+        _lib.call("pgb_coil_compress_tc", raw.data_ptr(), N, N_COILS_RAW, N_COILS, 1, mat.data_ptr(), out.data_ptr(),
+                  st)
+        ev[1].record()
+        torch.cuda.synchronize(dev)
+        if it >= 2:
+            ts.append(ev[0].elapsed_time(ev[1]))
+    ms_tc = float(np.median(ts))
+    err_tc = float((out - ref).norm() / ref.norm())
+    nbytes = N * (N_COILS_RAW + N_COILS) * 8
+    peak, kind = _peaks()
+    gbs, gbs_tc = nbytes / (ms / 1e3) / 1e9, nbytes / (ms_tc / 1e3) / 1e9
+    del raw, out, ref
+    return {"coils": [N_COILS_RAW, N_COILS], "samples": N, "algorithmic_bytes": nbytes,
+            "fp32": {"kernel": "coil_compress_kernel<32>", "ms": ms, "achieved_gbs": gbs, "roofline_frac": gbs / peak},
+            "bf16x3": {"kernel": "coil_compress_tc_kernel<32,2>", "ms": ms_tc, "achieved_gbs": gbs_tc,
+                       "roofline_frac": gbs_tc / peak, "rel_err_vs_fp32_kernel": err_tc},
+            "peak_source": kind, "fit_s_incl_fp64_covariance": fit_s}
+
+
 def cpu_baseline(coords, acr, spokes: int):
     """Reference CPU implementation timed on a bounded sample of the trajectory."""
     from oracle.ref_cpu import ReferenceCPU
@@ -626,6 +677,14 @@ def main():
         g.gridder_mode, g.gridder_brick, g._brick_plans = saved_mode, None, None
         torch.cuda.empty_cache()
 
+    coilc = None
+    if ws == 1 and not resized:
+        try:
+            coilc = coil_compress_c1(dev)
+        except Exception as exc:  # noqa: BLE001
+            coilc = {"error": f"{type(exc).__name__}: {exc}"}
+        torch.cuda.empty_cache()
+
     serving = cg2 = c3 = None
     if ws == 1 and args.serve_seconds > 0 and not resized:
         try:
@@ -683,6 +742,7 @@ def main():
             "gpu_launches": n_launch * args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "coil_compress_c1": coilc,
             "cg_sense_c2": cg2,
             "c3_batch": c3,
             "serving": serving,

@@ -375,6 +375,26 @@ PGB_API int pgb_grog_tc_use_tma(int64_t enable);
  * Synchronous.  No reference counterpart (diagnostics). */
 PGB_API int pgb_grog_tc_timeouts(int64_t* count, int64_t reset);
 
+/* =====================================================================
+ * Coil compression (the step before the path)
+ * ===================================================================== */
+
+/* cov (C, C) complex128 <- sum_m data[i, m] conj(data[j, m]) over the M
+ * samples of data (C, M) complex64 (coil-major), accumulated in FP64.  The
+ * covariance whose leading eigenvectors are the compression matrix of
+ * replaces: utils/_coil_compress.py:23-57 (coil_compress, which forwards to
+ * mrinufft's coil_compression).  C <= 32. */
+PGB_API int pgb_coil_covariance(const void* data, int64_t M, int64_t C, void* cov, void* stream);
+/* out (B, K, N) complex64 <- mat (K, C) complex64 @ data (B, C, N): the
+ * compression step of the same function.  1 <= K <= C <= 64. */
+PGB_API int pgb_coil_compress(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat,
+                              void* out, void* stream);
+/* The same product on the tensor cores (mma.sync bf16x3, FP32 accumulate,
+ * ~1e-5 relative): the matrix as register-resident A fragments, 8 samples x
+ * all coils per B fragment.  1 <= K <= min(C, 16), C <= 32. */
+PGB_API int pgb_coil_compress_tc(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat,
+                                 void* out, void* stream);
+
 /* Replica expansion of interpolate() (calib/_grog.py:668-695):
  * out[b,co,n*kw+j] = sum_ci T[interp_idx[n*kw+j],co,ci] * data[b,ci,n]
  * data (B,C,N), out (B,C,N*kw); entries outside [0,K) give 0. C <= 32. */

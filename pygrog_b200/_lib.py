@@ -142,6 +142,9 @@ _SIGS = {
     "pgb_grog_tc_blocks_per_sm": [_i64, _i64],
     "pgb_grog_tc_use_tma": [_i64],
     "pgb_grog_tc_timeouts": [_vp, _i64],
+    "pgb_coil_covariance": [_vp, _i64, _i64, _vp, _vp],
+    "pgb_coil_compress": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
+    "pgb_coil_compress_tc": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
 }
 _SIZE_FUNCS = {
     "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],

@@ -1,0 +1,274 @@
+// coil.cu -- PCA coil compression, the step before the GROG path.
+//
+// The reference's utils/_coil_compress.py:23-57 (coil_compress) forwards to
+// mrinufft's coil_compression: principal components of the multi-coil k-space
+// (optionally only the samples near the k-space centre) give a (K, C)
+// compression matrix, and the virtual coils are that matrix times the data.
+// Here the covariance of the calibration samples is accumulated in FP64 on
+// the device (pgb_coil_covariance), its eigendecomposition is a C x C host
+// problem, and the compression itself (pgb_coil_compress) is one HBM-bound
+// pass: every sample's C coils are read once, its K virtual coils written once.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace pgb {
+namespace coil {
+
+constexpr int kChunk = 64;   // samples per shared-memory chunk of the covariance
+constexpr int kCovT = 256;   // threads of the covariance kernel
+
+// cov[i * C + j] += sum_m D[i, m] conj(D[j, m]) over this block's sample chunks
+// (D coil-major (C, M) complex64, accumulation in FP64).
+__global__ void __launch_bounds__(kCovT) coil_cov_kernel(const float2* __restrict__ D, int64_t M, int C,
+                                                         double2* __restrict__ cov) {
+  __shared__ float2 tile[32][kChunk + 1];
+  const int tid = threadIdx.x;
+  const int pairs = C * C;
+  double2 acc[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) acc[k] = make_double2(0.0, 0.0);
+  for (int64_t m0 = static_cast<int64_t>(blockIdx.x) * kChunk; m0 < M;
+       m0 += static_cast<int64_t>(gridDim.x) * kChunk) {
+    for (int e = tid; e < C * kChunk; e += kCovT) {
+      const int c = e / kChunk;
+      const int s = e - c * kChunk;
+      tile[c][s] = m0 + s < M ? D[static_cast<int64_t>(c) * M + m0 + s] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = tid + k * kCovT;
+      if (p < pairs) {
+        const int i = p / C;
+        const int j = p - i * C;
+        double2 a = acc[k];
+        for (int s = 0; s < kChunk; ++s) {
+          const float2 u = tile[i][s], v = tile[j][s];
+          a.x = fma(static_cast<double>(u.x), static_cast<double>(v.x), a.x);
+          a.x = fma(static_cast<double>(u.y), static_cast<double>(v.y), a.x);
+          a.y = fma(static_cast<double>(u.y), static_cast<double>(v.x), a.y);
+          a.y = fma(-static_cast<double>(u.x), static_cast<double>(v.y), a.y);
+        }
+        acc[k] = a;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int p = tid + k * kCovT;
+    if (p < pairs) {
+      atomicAdd(&cov[p].x, acc[k].x);
+      atomicAdd(&cov[p].y, acc[k].y);
+    }
+  }
+}
+
+__global__ void zero_f64(double2* __restrict__ p, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = make_double2(0.0, 0.0);
+}
+
+// out[b, k, n] = sum_c mat[k, c] data[b, c, n]; one thread per sample, the
+// sample's coils in registers, the matrix in shared memory (broadcast reads).
+template <int CMAX>
+__global__ void __launch_bounds__(256) coil_compress_kernel(const float2* __restrict__ data, int64_t N, int C, int K,
+                                                            int B, const float2* __restrict__ mat,
+                                                            float2* __restrict__ out) {
+  extern __shared__ float2 ms[];
+  for (int i = threadIdx.x; i < K * C; i += blockDim.x) ms[i] = mat[i];
+  __syncthreads();
+  const int64_t total = static_cast<int64_t>(B) * N;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = t / N;
+    const int64_t n = t - b * N;
+    const float2* src = data + b * C * N + n;
+    float2 x[CMAX];
+#pragma unroll
+    for (int c = 0; c < CMAX; ++c) x[c] = c < C ? __ldg(src + static_cast<int64_t>(c) * N) : make_float2(0.f, 0.f);
+    float2* dst = out + b * K * N + n;
+    for (int k = 0; k < K; ++k) {
+      const float2* row = ms + k * C;
+      float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int c = 0; c < CMAX; c += 2) {
+        if (c < C) cfma(a0, row[c], x[c]);
+        if (c + 1 < C) cfma(a1, row[c + 1], x[c + 1]);
+      }
+      dst[static_cast<int64_t>(k) * N] = make_float2(a0.x + a1.x, a0.y + a1.y);
+    }
+  }
+}
+
+// ---- tensor-core compression ---------------------------------------------------
+// out = mat @ data as D (2 KP x 8 samples) = A (2 KP x 2 CIP) B (2 CIP x 8): A is
+// the realified matrix with rows [Re out 0..7 | Im out 0..7] per 16-row tile, so
+// a lane's two accumulator rows g and g + 8 are the real and imaginary parts of
+// output coil g; B is 8 samples with (re, im) of every input coil interleaved
+// along k, loaded straight from the coil planes (8 samples x 4 coils per load).
+// bf16x3: A = Ah + Al, B = Bh + Bl, D = Al Bh + Ah Bl + Ah Bh in FP32.
+__device__ __forceinline__ void mma16c(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint32_t bf2(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ void split_bf2(float x, float y, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x, y);
+  const float2 hf = __bfloat1622float2(h);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = bf2(x - hf.x, y - hf.y);
+}
+
+template <int CIP, int KT>  // CIP input coils (multiple of 8), KT 16-row tiles (8 output coils each)
+__global__ void __launch_bounds__(256) coil_compress_tc_kernel(const float2* __restrict__ data, int64_t N, int C,
+                                                               int K, int B, const float2* __restrict__ mat,
+                                                               float2* __restrict__ out) {
+  constexpr int KC = CIP / 8;  // k16 chunks (8 input coils each)
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  // A fragments of the realified matrix, heads and tails:
+  // A[r][2c] = Re / Im part, A[r][2c + 1] = -Im / Re part (row r < 8: Re of out coil r, else Im)
+  uint32_t ah[KT][KC][4], al[KT][KC][4];
+#pragma unroll
+  for (int T = 0; T < KT; ++T)
+#pragma unroll
+    for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int row = g + ((q & 1) ? 8 : 0);       // a0/a2: row g, a1/a3: row g + 8
+        const int c = 8 * kc + t + ((q & 2) ? 4 : 0);  // a0/a1: k cols 2t.., a2/a3: 2t + 8..
+        const int ko = 8 * T + (row & 7);
+        float2 m = make_float2(0.f, 0.f);
+        if (ko < K && c < C) m = __ldg(mat + ko * C + c);
+        const float e0 = row < 8 ? m.x : m.y;   // times x_re
+        const float e1 = row < 8 ? -m.y : m.x;  // times x_im
+        split_bf2(e0, e1, ah[T][kc][q], al[T][kc][q]);
+      }
+  const int64_t tiles = (N + 7) / 8;
+  const int64_t total = static_cast<int64_t>(B) * tiles;
+  const int64_t warp_id = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t n_warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t w = warp_id; w < total; w += n_warps) {
+    const int64_t b = w / tiles;
+    const int64_t n0 = (w - b * tiles) * 8;
+    const int64_t n = n0 + g;  // this lane's sample in the B fragment
+    const float2* src = data + b * C * N;
+    uint32_t bh[KC][2], bl[KC][2];
+#pragma unroll
+    for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = 8 * kc + t + 4 * h;
+        const float2 x = (n < N && c < C) ? __ldg(src + static_cast<int64_t>(c) * N + n) : make_float2(0.f, 0.f);
+        split_bf2(x.x, x.y, bh[kc][h], bl[kc][h]);
+      }
+#pragma unroll
+    for (int T = 0; T < KT; ++T) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int kc = 0; kc < KC; ++kc) {
+        mma16c(d, al[T][kc], bh[kc][0], bh[kc][1]);
+        mma16c(d, ah[T][kc], bl[kc][0], bl[kc][1]);
+        mma16c(d, ah[T][kc], bh[kc][0], bh[kc][1]);
+      }
+      // d[0], d[1]: Re of out coil 8T + g at samples 2t, 2t + 1; d[2], d[3]: Im
+      const int ko = 8 * T + g;
+      if (ko < K) {
+        float2* dst = out + (b * K + ko) * N + n0 + 2 * t;
+        if (n0 + 2 * t < N) dst[0] = make_float2(d[0], d[2]);
+        if (n0 + 2 * t + 1 < N) dst[1] = make_float2(d[1], d[3]);
+      }
+    }
+  }
+}
+
+}  // namespace coil
+}  // namespace pgb
+
+using namespace pgb;
+using namespace pgb::coil;
+
+extern "C" {
+
+int pgb_coil_covariance(const void* data, int64_t M, int64_t C, void* cov, void* stream) {
+  const char* who = "coil_covariance";
+  clear_error();
+  PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED, "%s: 1..32 coils, got %lld", who, (long long)C);
+  PGB_REQUIRE(M >= 0, PGB_ERR_INVALID, "%s: negative sample count", who);
+  PGB_REQUIRE(cov != nullptr && (data != nullptr || M == 0), PGB_ERR_INVALID, "%s: null pointer", who);
+  cudaStream_t s = as_stream(stream);
+  const int pairs = static_cast<int>(C * C);
+  zero_f64<<<(pairs + 255) / 256, 256, 0, s>>>(static_cast<double2*>(cov), pairs);
+  PGB_LAUNCH_CHECK(who);
+  if (M == 0) return PGB_OK;
+  const int blocks = grid_for((M + kChunk - 1) / kChunk, 1, 148 * 8);
+  coil_cov_kernel<<<blocks, kCovT, 0, s>>>(static_cast<const float2*>(data), M, static_cast<int>(C),
+                                          static_cast<double2*>(cov));
+  PGB_LAUNCH_CHECK(who);
+  return PGB_OK;
+}
+
+int pgb_coil_compress(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat, void* out,
+                      void* stream) {
+  const char* who = "coil_compress";
+  clear_error();
+  PGB_REQUIRE(C >= 1 && C <= 64, PGB_ERR_UNSUPPORTED, "%s: 1..64 coils, got %lld", who, (long long)C);
+  PGB_REQUIRE(K >= 1 && K <= C, PGB_ERR_INVALID, "%s: need 1 <= K <= C, got K=%lld C=%lld", who, (long long)K,
+              (long long)C);
+  PGB_REQUIRE(N >= 0 && B >= 0, PGB_ERR_INVALID, "%s: negative size", who);
+  if (N == 0 || B == 0) return PGB_OK;
+  PGB_REQUIRE(data && mat && out, PGB_ERR_INVALID, "%s: null pointer", who);
+  cudaStream_t s = as_stream(stream);
+  const size_t smem = static_cast<size_t>(K * C) * sizeof(float2);
+  const int blocks = grid_for(B * N, 256, 148 * 8);
+  if (C <= 32) {
+    coil_compress_kernel<32><<<blocks, 256, smem, s>>>(static_cast<const float2*>(data), N, static_cast<int>(C),
+                                                       static_cast<int>(K), static_cast<int>(B),
+                                                       static_cast<const float2*>(mat), static_cast<float2*>(out));
+  } else {
+    coil_compress_kernel<64><<<blocks, 256, smem, s>>>(static_cast<const float2*>(data), N, static_cast<int>(C),
+                                                       static_cast<int>(K), static_cast<int>(B),
+                                                       static_cast<const float2*>(mat), static_cast<float2*>(out));
+  }
+  PGB_LAUNCH_CHECK(who);
+  return PGB_OK;
+}
+
+int pgb_coil_compress_tc(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat, void* out,
+                         void* stream) {
+  const char* who = "coil_compress_tc";
+  clear_error();
+  PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED, "%s: 1..32 coils, got %lld", who, (long long)C);
+  PGB_REQUIRE(K >= 1 && K <= C && K <= 16, PGB_ERR_INVALID, "%s: need 1 <= K <= min(C, 16), got K=%lld", who,
+              (long long)K);
+  PGB_REQUIRE(N >= 0 && B >= 0, PGB_ERR_INVALID, "%s: negative size", who);
+  if (N == 0 || B == 0) return PGB_OK;
+  PGB_REQUIRE(data && mat && out, PGB_ERR_INVALID, "%s: null pointer", who);
+  cudaStream_t s = as_stream(stream);
+  const int64_t warps = B * ((N + 7) / 8);
+  const int blocks = grid_for(warps * 32, 256, 148 * 8);
+  const int cip = static_cast<int>((C + 7) / 8 * 8);
+  const int kt = K > 8 ? 2 : 1;
+  const float2* d = static_cast<const float2*>(data);
+  const float2* m = static_cast<const float2*>(mat);
+  float2* o = static_cast<float2*>(out);
+  const int Ci = static_cast<int>(C), Ki = static_cast<int>(K), Bi = static_cast<int>(B);
+  switch (cip * 10 + kt) {
+#define X(CI, KTT) \
+  case CI * 10 + KTT: coil_compress_tc_kernel<CI, KTT><<<blocks, 256, 0, s>>>(d, N, Ci, Ki, Bi, m, o); break;
+    X(8, 1) X(16, 1) X(16, 2) X(24, 1) X(24, 2) X(32, 1) X(32, 2)
+#undef X
+    default:
+      PGB_REQUIRE(false, PGB_ERR_UNSUPPORTED, "%s: no kernel for C=%lld K=%lld", who, (long long)C, (long long)K);
+  }
+  PGB_LAUNCH_CHECK(who);
+  return PGB_OK;
+}
+
+}  // extern "C"
