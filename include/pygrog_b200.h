@@ -385,6 +385,13 @@ PGB_API int pgb_grog_tc_timeouts(int64_t* count, int64_t reset);
  * replaces: utils/_coil_compress.py:23-57 (coil_compress, which forwards to
  * mrinufft's coil_compression).  C <= 32. */
 PGB_API int pgb_coil_covariance(const void* data, int64_t M, int64_t C, void* cov, void* stream);
+/* cov (C, C) complex128 <- sum_m data[i, m] conj(data2[j, m]) (FP64): the
+ * Gram matrices of the Tikhonov least squares of the unit GROG operators,
+ * src^H src and src^H dst over neighbour pairs of the calibration block
+ * (replaces the O(samples) part of calib/_grappa.py:16-59, lstsq, in the GPU
+ * table fit).  C <= 32. */
+PGB_API int pgb_coil_cross_covariance(const void* data, const void* data2, int64_t M, int64_t C, void* cov,
+                                      void* stream);
 /* out (B, K, N) complex64 <- mat (K, C) complex64 @ data (B, C, N): the
  * compression step of the same function.  1 <= K <= C <= 64. */
 PGB_API int pgb_coil_compress(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat,

@@ -143,6 +143,7 @@ _SIGS = {
     "pgb_grog_tc_use_tma": [_i64],
     "pgb_grog_tc_timeouts": [_vp, _i64],
     "pgb_coil_covariance": [_vp, _i64, _i64, _vp, _vp],
+    "pgb_coil_cross_covariance": [_vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_coil_compress": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
     "pgb_coil_compress_tc": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
 }

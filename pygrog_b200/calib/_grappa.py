@@ -80,13 +80,54 @@ def _unit_operators(calib: torch.Tensor, lamda: float) -> list[torch.Tensor]:
     return ops
 
 
-def train_grappa(train_data, lamda: float | None = None) -> SimpleNamespace:
-    """Unit GROG operators ``x``, ``y`` (and ``z`` in 3-D) from a Cartesian ACR."""
+def _unit_operators_device(calib: torch.Tensor, lamda: float, device) -> list[torch.Tensor]:
+    """The unit operators of :func:`_unit_operators` fitted in FP64 with the
+    O(samples) work on the GPU: the Gram matrices ``src^H src`` and
+    ``src^H dst`` of every axis's neighbour pairs are accumulated in FP64 by
+    ``pgb_coil_cross_covariance``; the regularised ``C x C`` normal equations
+    ``(src^H src + lamda I) X = src^H dst`` (the calibration block scaled to
+    unit norm, as in the reference) are solved on the host in FP64.  The
+    samples enter as complex64 (k-space calibration data).  The
+    least-squares solution equals the augmented-system one of
+    ``_grappa.py:16-59`` up to FP64 rounding (the regularised Gram matrix has
+    condition number <= 1 / lamda + 1)."""
+    from .. import _lib
+
+    dev = torch.device(device)
+    cal = torch.as_tensor(calib).to(dev)
+    norm2 = float(torch.linalg.norm(cal.to(torch.complex128)) ** 2)
+    cal = cal.to(torch.complex64)
+    nc = int(cal.shape[0])
+    st = _lib.stream_ptr(dev)
+    ops = []
+    for axis in range(1, cal.ndim):
+        m = cal.shape[axis] - 1
+        # (C, M) coil-major copies of the source and target samples of this axis
+        src = cal.narrow(axis, 0, m).reshape(nc, -1).contiguous()
+        dst = cal.narrow(axis, 1, m).reshape(nc, -1).contiguous()
+        M = int(src.shape[1])
+        g_ss = torch.empty(nc, nc, dtype=torch.complex128, device=dev)
+        g_sd = torch.empty(nc, nc, dtype=torch.complex128, device=dev)
+        _lib.call("pgb_coil_cross_covariance", src.data_ptr(), src.data_ptr(), M, nc, g_ss.data_ptr(), st)
+        _lib.call("pgb_coil_cross_covariance", src.data_ptr(), dst.data_ptr(), M, nc, g_sd.data_ptr(), st)
+        # kernel: sum_m a[i, m] conj(b[j, m]); src^H src = its conjugate, likewise src^H dst
+        A = g_ss.cpu().conj() / norm2 + lamda * torch.eye(nc, dtype=torch.complex128)
+        Bm = g_sd.cpu().conj() / norm2
+        X = torch.linalg.solve(A, Bm)
+        ops.append(X.mT)
+    return ops
+
+
+def train_grappa(train_data, lamda: float | None = None, device=None) -> SimpleNamespace:
+    """Unit GROG operators ``x``, ``y`` (and ``z`` in 3-D) from a Cartesian ACR.
+
+    With ``device`` (a CUDA device) the fit runs in FP64 with its Gram
+    matrices accumulated on that GPU (:func:`_unit_operators_device`)."""
     if lamda is None:
         lamda = 0.01
     t = torch.as_tensor(train_data)
     ndim = t.ndim - 1
-    ops = _unit_operators(t, lamda)
+    ops = _unit_operators_device(t, lamda, device) if device is not None else _unit_operators(t, lamda)
     if ndim == 2:
         return SimpleNamespace(x=ops[0], y=ops[1], z=None)
     if ndim == 3:
@@ -142,20 +183,27 @@ def KernelTable(
     lamda: float = 0.01,
     fit_dtype: torch.dtype | None = None,
     return_factors: bool = False,
+    fit_device=None,
 ):
     """Return ``(table (nsteps**ndim, C, C) ndarray, nsteps, ndim)``.
 
     ``fit_dtype`` (e.g. ``torch.complex128``) runs the least squares, logm and
     expm in that precision and casts the table back to the ACR's dtype.
     With ``return_factors`` a fourth item ``(outer, inner)`` is returned (see
-    :func:`table_factors`), cast like the table.
+    :func:`table_factors`), cast like the table.  ``fit_device`` (a CUDA
+    device) fits the unit operators in FP64 on that GPU
+    (:func:`_unit_operators_device`); the powers and the product follow in
+    FP64 on the host.
     """
     t = torch.as_tensor(np.asarray(train_data)) if isinstance(train_data, np.ndarray) else torch.as_tensor(train_data)
     t = t.detach().cpu()
     out_dtype = t.dtype if t.is_complex() else torch.complex64
-    if fit_dtype is not None:
+    if fit_device is not None and t.dtype == torch.complex128:
+        fit_device = None  # complex128 calibration data: the host FP64 fit keeps every bit
+        fit_dtype = torch.complex128
+    if fit_dtype is not None and fit_device is None:
         t = t.to(fit_dtype)
-    ops = train_grappa(t, lamda)
+    ops = train_grappa(t, lamda, device=fit_device)
     _, nsteps, deltas = shift_steps(radius, precision)
     Gx = grappa_power(ops.x, deltas)
     Gy = grappa_power(ops.y, deltas)

@@ -864,15 +864,19 @@ class GrogInterpolator:
         return self.plan
 
     # -- table ----------------------------------------------------------------
-    def calc_interp_table(self, train_data, lamda: float = 0.01, precision: int = 1, *, fit_dtype=None):
+    def calc_interp_table(self, train_data, lamda: float = 0.01, precision: int = 1, *, fit_dtype=None,
+                          fit_on_device: bool = False):
         """Fit the GRAPPA shift table and quantise every replica's shift.
 
-        ``fit_dtype=torch.complex128`` runs the fit in FP64 (table cast back).
+        ``fit_dtype=torch.complex128`` runs the fit in FP64 (table cast back);
+        ``fit_on_device=True`` runs it in FP64 with the least-squares Gram
+        matrices accumulated on this interpolator's GPU.
         """
         if isinstance(train_data, torch.Tensor):
             train_data = train_data.detach().cpu()
         table, nsteps, ndim, factors = KernelTable(
-            train_data, self.plan.radius, precision, lamda, fit_dtype, return_factors=True
+            train_data, self.plan.radius, precision, lamda, fit_dtype, return_factors=True,
+            fit_device=self.device if fit_on_device else None,
         )
         self._factors = factors
         self._nsteps = int(nsteps)

@@ -18,11 +18,13 @@ namespace coil {
 constexpr int kChunk = 64;   // samples per shared-memory chunk of the covariance
 constexpr int kCovT = 256;   // threads of the covariance kernel
 
-// cov[i * C + j] += sum_m D[i, m] conj(D[j, m]) over this block's sample chunks
-// (D coil-major (C, M) complex64, accumulation in FP64).
-__global__ void __launch_bounds__(kCovT) coil_cov_kernel(const float2* __restrict__ D, int64_t M, int C,
-                                                         double2* __restrict__ cov) {
+// cov[i * C + j] += sum_m D[i, m] conj(E[j, m]) over this block's sample chunks
+// (D, E coil-major (C, M) complex64, accumulation in FP64; E == D for a
+// covariance).
+__global__ void __launch_bounds__(kCovT) coil_cov_kernel(const float2* __restrict__ D, const float2* __restrict__ E,
+                                                         int64_t M, int C, double2* __restrict__ cov) {
   __shared__ float2 tile[32][kChunk + 1];
+  __shared__ float2 tile_e[32][kChunk + 1];
   const int tid = threadIdx.x;
   const int pairs = C * C;
   double2 acc[4];
@@ -34,6 +36,7 @@ __global__ void __launch_bounds__(kCovT) coil_cov_kernel(const float2* __restric
       const int c = e / kChunk;
       const int s = e - c * kChunk;
       tile[c][s] = m0 + s < M ? D[static_cast<int64_t>(c) * M + m0 + s] : make_float2(0.f, 0.f);
+      tile_e[c][s] = m0 + s < M ? E[static_cast<int64_t>(c) * M + m0 + s] : make_float2(0.f, 0.f);
     }
     __syncthreads();
 #pragma unroll
@@ -44,7 +47,7 @@ __global__ void __launch_bounds__(kCovT) coil_cov_kernel(const float2* __restric
         const int j = p - i * C;
         double2 a = acc[k];
         for (int s = 0; s < kChunk; ++s) {
-          const float2 u = tile[i][s], v = tile[j][s];
+          const float2 u = tile[i][s], v = tile_e[j][s];
           a.x = fma(static_cast<double>(u.x), static_cast<double>(v.x), a.x);
           a.x = fma(static_cast<double>(u.y), static_cast<double>(v.y), a.x);
           a.y = fma(static_cast<double>(u.y), static_cast<double>(v.x), a.y);
@@ -196,22 +199,27 @@ using namespace pgb::coil;
 
 extern "C" {
 
-int pgb_coil_covariance(const void* data, int64_t M, int64_t C, void* cov, void* stream) {
-  const char* who = "coil_covariance";
+int pgb_coil_cross_covariance(const void* data, const void* data2, int64_t M, int64_t C, void* cov, void* stream) {
+  const char* who = "coil_cross_covariance";
   clear_error();
   PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED, "%s: 1..32 coils, got %lld", who, (long long)C);
   PGB_REQUIRE(M >= 0, PGB_ERR_INVALID, "%s: negative sample count", who);
-  PGB_REQUIRE(cov != nullptr && (data != nullptr || M == 0), PGB_ERR_INVALID, "%s: null pointer", who);
+  PGB_REQUIRE(cov != nullptr && ((data != nullptr && data2 != nullptr) || M == 0), PGB_ERR_INVALID,
+              "%s: null pointer", who);
   cudaStream_t s = as_stream(stream);
   const int pairs = static_cast<int>(C * C);
   zero_f64<<<(pairs + 255) / 256, 256, 0, s>>>(static_cast<double2*>(cov), pairs);
   PGB_LAUNCH_CHECK(who);
   if (M == 0) return PGB_OK;
   const int blocks = grid_for((M + kChunk - 1) / kChunk, 1, 148 * 8);
-  coil_cov_kernel<<<blocks, kCovT, 0, s>>>(static_cast<const float2*>(data), M, static_cast<int>(C),
-                                          static_cast<double2*>(cov));
+  coil_cov_kernel<<<blocks, kCovT, 0, s>>>(static_cast<const float2*>(data), static_cast<const float2*>(data2), M,
+                                          static_cast<int>(C), static_cast<double2*>(cov));
   PGB_LAUNCH_CHECK(who);
   return PGB_OK;
+}
+
+int pgb_coil_covariance(const void* data, int64_t M, int64_t C, void* cov, void* stream) {
+  return pgb_coil_cross_covariance(data, data, M, C, cov, stream);
 }
 
 int pgb_coil_compress(const void* data, int64_t N, int64_t C, int64_t K, int64_t B, const void* mat, void* out,

@@ -252,3 +252,19 @@ def test_autotuner_picks_a_valid_gridder(cuda):
     clear_cache()
     strict = autotune_gridder(g, tolerance=1e-6, reps=1)
     assert all(t[0] in ("v8", "v6") for t in strict["trials"])
+
+
+@pytest.mark.parametrize("case", golden_plan_cases())
+def test_device_table_fit_matches_host_fp64_fit(cuda, case):
+    """Table fit with the least-squares Gram matrices accumulated on the GPU in
+    FP64: equal to the host FP64 fit, and within the FP32-vs-FP64 fit spread
+    of the reference's own table."""
+    from pygrog_b200.calib import _grappa
+
+    z = golden(case)
+    name, shape, osf, kwd, ks, prec, C = parse_meta(z["meta"])
+    t64, _, _ = _grappa.KernelTable(z["in_calib"], 0.5, prec, 0.01, fit_dtype=torch.complex128)
+    td, _, _ = _grappa.KernelTable(z["in_calib"], 0.5, prec, 0.01, fit_device=cuda)
+    assert td.dtype == np.complex64
+    assert rel_l2(td, t64) < 1e-6
+    assert rel_l2(td[z["ref_table_used_idx"]], z["ref_table_used"]) < 1e-4
