@@ -268,3 +268,42 @@ def test_device_table_fit_matches_host_fp64_fit(cuda, case):
     assert td.dtype == np.complex64
     assert rel_l2(td, t64) < 1e-6
     assert rel_l2(td[z["ref_table_used_idx"]], z["ref_table_used"]) < 1e-4
+
+
+def test_tensor_core_stacked_batched_and_interpolate_grid(cuda):
+    """tc mode on a stacked plan with a (B,) batch equals the per-stack
+    interpolators (same kernels), and interpolate(grid=True) in tc mode returns
+    the tc grid with the density / mask of the FP32 path."""
+    from pygrog_b200.workloads import radial2d
+
+    rng = np.random.default_rng(2)
+    co = np.stack([radial2d(12, 64, 16.0), radial2d(12, 64, 16.0)[:, ::-1]])  # (S=2, 12, 64, 2)
+    calib = (rng.standard_normal((8, 8, 8)) + 1j * rng.standard_normal((8, 8, 8))).astype(np.complex64)
+    g = GrogInterpolator(shape=(32, 32), coords=co, oversamp=2.0, kernel_width=2, device=cuda)
+    g.calc_interp_table(calib)
+    g.gridder_mode = "tc"
+    data = (rng.standard_normal((3, 2, 8, 12, 64)) + 1j * rng.standard_normal((3, 2, 8, 12, 64))).astype(np.complex64)
+    kg = g.grid(data)
+    back = g.degrid(kg)
+    assert kg.shape == (3, 2, 8, 64, 64) and back.shape == data.shape
+    for s in range(2):
+        gs = GrogInterpolator(shape=(32, 32), coords=co[s], oversamp=2.0, kernel_width=2, device=cuda)
+        gs.calc_interp_table(calib)
+        gs.gridder_mode = "tc"
+        assert rel_l2(kg[:, s], gs.grid(data[:, s])) < 1e-6
+        assert rel_l2(back[:, s], gs.degrid(kg[:, s])) < 1e-6
+        # against the FP64 oracle
+        table = gs._interp_kernel.numpy().astype(np.complex128)
+        p = og.create_plan((32, 32), co[s], 2.0, 2, "circle")
+        qi = gs._interp_idx.cpu().numpy()
+        ref, _ = og.grid(data[:, s].reshape(3, 8, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
+        assert rel_l2(kg[:, s].reshape(3, 8, -1), ref) < 1e-4
+    g1 = GrogInterpolator(shape=(32, 32), coords=co[0], oversamp=2.0, kernel_width=2, device=cuda)
+    g1.calc_interp_table(calib)
+    kg32, mp32 = g1.interpolate(data[0, 0], grid=True)
+    g1.gridder_mode = "tc"
+    g1._brick_plans = None
+    kgt, mpt = g1.interpolate(data[0, 0], grid=True)
+    assert rel_l2(kgt, kg32) < 1e-4
+    np.testing.assert_array_equal(np.asarray(mpt.mask), np.asarray(mp32.mask))
+    np.testing.assert_allclose(np.asarray(mpt.density), np.asarray(mp32.density), rtol=1e-6)
