@@ -463,6 +463,10 @@ class GrogGridder:
     """Fused GROG gridding operator for one trajectory: brick plans + tables.
 
     Kernel families (chosen from the shared-memory budget of one CTA):
+      ``"tc"``        C <= 32: eigen-factored table as a chain of dense
+                      coil matrices on the tensor cores (bf16x3 split
+                      products, FP32 accumulate) with per-replica phases;
+      ``"tc1"``       the same chain with plain bf16 products;
       ``"v8"``        C <= 16: one lane per replica on balanced sub-chunk
                       streams, replicas ordered (outer, inner, cell) so
                       operator loads are conflict-free or broadcast; the
@@ -667,8 +671,9 @@ class GrogGridder:
         C = self.C
         if tc_ops is None:
             raise ValueError("tensor-core gridding needs the eigen-factored table (calc_interp_table first)")
-        if C > 16:
-            raise ValueError("tc kernels cover C <= 16")
+        if C > 32:
+            raise ValueError("tc kernels cover C <= 32")
+        cap = 256 if C <= 16 else 128  # one m-tile per warp above 16 coils
         nd, nsteps = int(tc_ops["ndim"]), int(tc_ops["nsteps"])
         if nd != len(grid_shape):
             raise ValueError("table and plan dimensionality differ")
@@ -677,21 +682,21 @@ class GrogGridder:
         chosen = None
         for br in cand:
             cells = br[0] * br[1] * br[2]
-            if lib.pgb_grog_tc_smem_bytes(C, cells, nsteps, nd, 256) <= budget:
+            if lib.pgb_grog_tc_smem_bytes(C, cells, nsteps, nd, cap) <= budget:
                 chosen = tuple(br)
                 break
         if chosen is None:
             raise ValueError("tc kernels: no brick fits shared memory")
         self.mode = mode
         self.brick = chosen
-        self.sub_cap = 256
+        self.sub_cap = cap
         self.tc = tc_ops
         self.terms = 3 if mode == "tc" else 1
         self.n_outer = nsteps
         self.fwd6 = None
         self.pairs = False
         dev = target_idx.device
-        kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=256, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True,
+        kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=cap, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True,
                    full_subs=True)
         self.plan = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, cell_rows=True,
                                pack_rows=self.PACK_ROWS_TC, **kwt)

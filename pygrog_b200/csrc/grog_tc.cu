@@ -52,7 +52,7 @@
 namespace pgb {
 namespace tc {
 
-constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk
+constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk (128 above 16 coils)
 constexpr int kFirst = 1, kLast = 2, kSplit = 4;
 
 template <int CP>
@@ -61,7 +61,12 @@ struct Shape {
   static constexpr int K16 = NT / 2;                  // k16 chunks of the next stage
   static constexpr int K8 = NT % 2;                   // trailing k8 chunk
   static constexpr int NFR = NT * (2 * K16 + K8);     // B-fragment words per lane per matrix
+  static constexpr int FPN = 2 * K16 + K8;            // words per n-tile
+  static constexpr int WQ = (FPN + 3) / 4;            // 16-byte groups per n-tile and head / tail
   static constexpr int TS = CP + 1;                   // tile stride per cell (float2): conflict-free flush
+  // m-tiles a warp runs side by side: two up to 16 coils (256-entry
+  // sub-chunks), one above (128-entry sub-chunks: the registers of one tile)
+  static constexpr int NTL = CP <= 16 ? 2 : 1;
 };
 
 template <int CP, int NS>
@@ -209,11 +214,12 @@ __device__ __forceinline__ void split2(float2 v, uint32_t& hi, uint32_t& lo) {
 // 16-byte word group of heads and one of tails per lane (lane-contiguous:
 // conflict-free).
 template <int CP, int TERMS>
-__device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const uint4* __restrict__ wst, int lane) {
+__device__ __forceinline__ void mm_stage(float2 (&v)[Shape<CP>::NTL][2][Shape<CP>::NT], const uint4* __restrict__ wst, int lane) {
   constexpr int NT = Shape<CP>::NT, K16 = Shape<CP>::K16, K8 = Shape<CP>::K8;
-  uint32_t ah[2][2][NT], al[2][2][NT];
+  constexpr int NTL = Shape<CP>::NTL, WQ = Shape<CP>::WQ;
+  uint32_t ah[NTL][2][NT], al[NTL][2][NT];
 #pragma unroll
-  for (int T = 0; T < 2; ++T)
+  for (int T = 0; T < NTL; ++T)
 #pragma unroll
     for (int r = 0; r < 2; ++r)
 #pragma unroll
@@ -227,14 +233,18 @@ __device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const
       }
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) {
-    const uint4 bh4 = wst[(nt * 2) * 32 + lane];
-    const uint4 bl4 = wst[(nt * 2 + 1) * 32 + lane];
-    const uint32_t bh[4] = {bh4.x, bh4.y, bh4.z, bh4.w};
-    const uint32_t bl[4] = {bl4.x, bl4.y, bl4.z, bl4.w};
-    // products alternate between two accumulators per tile (tails first)
-    float d[2][2][4];
+    uint32_t bh[4 * WQ], bl[4 * WQ];
 #pragma unroll
-    for (int T = 0; T < 2; ++T)
+    for (int q = 0; q < WQ; ++q) {
+      const uint4 h4 = wst[((nt * 2) * WQ + q) * 32 + lane];
+      const uint4 l4 = wst[((nt * 2 + 1) * WQ + q) * 32 + lane];
+      bh[4 * q] = h4.x, bh[4 * q + 1] = h4.y, bh[4 * q + 2] = h4.z, bh[4 * q + 3] = h4.w;
+      bl[4 * q] = l4.x, bl[4 * q + 1] = l4.y, bl[4 * q + 2] = l4.z, bl[4 * q + 3] = l4.w;
+    }
+    // products alternate between two accumulators per tile (tails first)
+    float d[NTL][2][4];
+#pragma unroll
+    for (int T = 0; T < NTL; ++T)
 #pragma unroll
       for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -245,18 +255,18 @@ __device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const
       const int f = 2 * kc;
       if constexpr (TERMS == 3) {
 #pragma unroll
-        for (int T = 0; T < 2; ++T)
+        for (int T = 0; T < NTL; ++T)
           mma16(d[T][q & 1], al[T][0][2 * kc], al[T][1][2 * kc], al[T][0][2 * kc + 1], al[T][1][2 * kc + 1], bh[f],
                 bh[f + 1]);
         ++q;
 #pragma unroll
-        for (int T = 0; T < 2; ++T)
+        for (int T = 0; T < NTL; ++T)
           mma16(d[T][q & 1], ah[T][0][2 * kc], ah[T][1][2 * kc], ah[T][0][2 * kc + 1], ah[T][1][2 * kc + 1], bl[f],
                 bl[f + 1]);
         ++q;
       }
 #pragma unroll
-      for (int T = 0; T < 2; ++T)
+      for (int T = 0; T < NTL; ++T)
         mma16(d[T][q & 1], ah[T][0][2 * kc], ah[T][1][2 * kc], ah[T][0][2 * kc + 1], ah[T][1][2 * kc + 1], bh[f],
               bh[f + 1]);
       ++q;
@@ -265,17 +275,17 @@ __device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const
       const int f = 2 * K16;
       if constexpr (TERMS == 3) {
 #pragma unroll
-        for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], al[T][0][NT - 1], al[T][1][NT - 1], bh[f]);
+        for (int T = 0; T < NTL; ++T) mma8(d[T][q & 1], al[T][0][NT - 1], al[T][1][NT - 1], bh[f]);
         ++q;
 #pragma unroll
-        for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bl[f]);
+        for (int T = 0; T < NTL; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bl[f]);
         ++q;
       }
 #pragma unroll
-      for (int T = 0; T < 2; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bh[f]);
+      for (int T = 0; T < NTL; ++T) mma8(d[T][q & 1], ah[T][0][NT - 1], ah[T][1][NT - 1], bh[f]);
     }
 #pragma unroll
-    for (int T = 0; T < 2; ++T) {
+    for (int T = 0; T < NTL; ++T) {
       v[T][0][nt] = make_float2(d[T][0][0] + d[T][1][0], d[T][0][1] + d[T][1][1]);
       v[T][1][nt] = make_float2(d[T][0][2] + d[T][1][2], d[T][0][3] + d[T][1][3]);
     }
@@ -286,15 +296,18 @@ __device__ __forceinline__ void mm_stage(float2 (&v)[2][2][Shape<CP>::NT], const
 // head/tail, lane, 4 words) from the global layout (stage, head/tail, word, lane).
 template <int CP, int NS>
 __device__ __forceinline__ void stage_w(uint32_t* __restrict__ wsm, const uint32_t* __restrict__ wfrag) {
-  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, FPN = NFR / NT;
-  constexpr int total = (NS + 1) * NT * 2 * 32 * 4;
-  for (int i = threadIdx.x; i < total; i += kT) {
-    const int w = i & 3;
+  constexpr int NT = Shape<CP>::NT, NFR = Shape<CP>::NFR, FPN = Shape<CP>::FPN, WQ = Shape<CP>::WQ;
+  constexpr int total = (NS + 1) * NT * 2 * WQ * 32 * 4;
+  for (int i = threadIdx.x; i < total; i += kT) {  // layout (stage, nt, head / tail, q, lane, 4 words)
+    const int w4 = i & 3;
     const int lane = (i >> 2) & 31;
-    const int b = (i >> 7) & 1;
-    const int snt = i >> 8;  // stage * NT + nt
+    const int r = i >> 7;  // ((stage * NT + nt) * 2 + b) * WQ + q
+    const int q = r % WQ;
+    const int b = (r / WQ) & 1;
+    const int snt = r / (WQ * 2);
     const int s = snt / NT;
     const int nt = snt - s * NT;
+    const int w = 4 * q + w4;
     wsm[i] = w < FPN ? __ldg(wfrag + ((s * 2 + b) * NFR + nt * FPN + w) * 32 + lane) : 0u;
   }
 }
@@ -335,17 +348,17 @@ __device__ __forceinline__ int diag_index(const Row& r, int s) {
 // The whole chain on a warp's two m-tiles: NS + 1 dense stages with the
 // diagonal phases of table dt (NS, nsteps, row stride dstride) between them.
 template <int CP, int NS, int TERMS, bool ADJ>
-__device__ __forceinline__ void chain(float2 (&v)[2][2][Shape<CP>::NT], const uint4* __restrict__ wsm,
+__device__ __forceinline__ void chain(float2 (&v)[Shape<CP>::NTL][2][Shape<CP>::NT], const uint4* __restrict__ wsm,
                                       const float2* __restrict__ dt, int nsteps, int dstride,
-                                      const Row (&rw)[2][2], int lane) {
-  constexpr int NT = Shape<CP>::NT;
+                                      const Row (&rw)[Shape<CP>::NTL][2], int lane) {
+  constexpr int NT = Shape<CP>::NT, NTL = Shape<CP>::NTL, WQ = Shape<CP>::WQ;
   const int t = lane & 3;
 #pragma unroll
   for (int s = 0; s <= NS; ++s) {
-    mm_stage<CP, TERMS>(v, wsm + s * NT * 2 * 32, lane);
+    mm_stage<CP, TERMS>(v, wsm + s * NT * 2 * WQ * 32, lane);
     if (s < NS) {
 #pragma unroll
-      for (int T = 0; T < 2; ++T)
+      for (int T = 0; T < NTL; ++T)
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
           const float2* drow = dt + (s * nsteps + diag_index<NS, ADJ>(rw[T][r], s)) * dstride + t;
@@ -446,8 +459,9 @@ struct Smem {
   __host__ __device__ Smem(int CP, int NS, int nsteps, int cells, int cap, bool forward, bool tma = false) {
     dt = 0;
     const Phases ph(CP, NS, nsteps);
-    wf = (ph.copies * ph.copy_sz + 1) & ~1;       // W fragments: (NS + 1) * (CP / 4) * 2 * 32 uint4
-    tile = wf + (NS + 1) * (CP / 4) * 2 * 32 * 2;  // float2 units
+    wf = (ph.copies * ph.copy_sz + 1) & ~1;       // W fragments: (NS + 1) * (CP / 4) * 2 * WQ * 32 uint4
+    const int wq = ((2 * (CP / 8) + (CP / 4) % 2) + 3) / 4;  // Shape<CP>::WQ
+    tile = wf + (NS + 1) * (CP / 4) * 2 * wq * 32 * 2;  // float2 units
     if (tma) {
       tile = (tile + 15) & ~15;  // 128-byte aligned TMA boxes, [coil][cell]
       tile_sz = (cells * CP + 15) & ~15;
@@ -671,11 +685,12 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       const float2* xs = xs0 + buf * lay.xs_sz;
       const int2* msb = ms0 + buf * cap;
       const float* wsb = ws0 + buf * cap;
-      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp and warp + 8
-        Row rw[2][2];
-        float2 v[2][2][NT];
+      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp (and warp + 8 up to 16 coils)
+        constexpr int NTL = Shape<CP>::NTL;
+        Row rw[NTL][2];
+        float2 v[NTL][2][NT];
 #pragma unroll
-        for (int T = 0; T < 2; ++T)
+        for (int T = 0; T < NTL; ++T)
 #pragma unroll
           for (int r = 0; r < 2; ++r) {
             const int e = (warp + 8 * T) * 16 + 2 * g + r;  // cell-ordered rows: entry 2 g + r on row g + 8 r
@@ -689,7 +704,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
           }
         chain<CP, NS, TERMS, false>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
 #pragma unroll
-        for (int T = 0; T < 2; ++T) {
+        for (int T = 0; T < NTL; ++T) {
           if ((warp + 8 * T) * 16 >= nr) break;  // warp-uniform
 #pragma unroll
           for (int r = 0; r < 2; ++r)
@@ -864,11 +879,12 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
       const float2* tl = tiles + par * lay.tile_sz;
       const int2* msb = ms0 + mb * cap;
       const float* wsb = ws0 + mb * cap;
-      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp and warp + 8
-        Row rw[2][2];
-        float2 v[2][2][NT];
+      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp (and warp + 8 up to 16 coils)
+        constexpr int NTL = Shape<CP>::NTL;
+        Row rw[NTL][2];
+        float2 v[NTL][2][NT];
 #pragma unroll
-        for (int T = 0; T < 2; ++T)
+        for (int T = 0; T < NTL; ++T)
 #pragma unroll
           for (int r = 0; r < 2; ++r) {
             const int e = (warp + 8 * T) * 16 + 8 * r + g;  // sample-ordered rows: entry 8 r + g on row g + 8 r
@@ -884,7 +900,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
           }
         chain<CP, NS, TERMS, true>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
 #pragma unroll
-        for (int T = 0; T < 2; ++T)
+        for (int T = 0; T < NTL; ++T)
 #pragma unroll
           for (int r = 0; r < 2; ++r) {
             if (!rw[T][r].on) continue;
@@ -963,7 +979,10 @@ __global__ void zero_samples_tc(float2* __restrict__ out, int64_t N, int C, int 
   }
 }
 
-inline int padded(int64_t C) { return static_cast<int>((C + 3) / 4 * 4); }
+// coil padding of the kernels: multiples of 4 up to 16, of 8 above (24, 32)
+inline int padded(int64_t C) { return static_cast<int>(C <= 16 ? (C + 3) / 4 * 4 : (C + 7) / 8 * 8); }
+// entries of one sub-chunk: 8 warps x 16 rows x the m-tiles a warp runs (Shape<CP>::NTL)
+inline int tc_rows(int64_t C) { return padded(C) <= 16 ? 2 * 8 * 16 : 8 * 16; }
 
 static int geom_of(const pgb_v6_plan* p, Geom& g, const char* who) {
   PGB_REQUIRE(p != nullptr, PGB_ERR_INVALID, "%s: null plan", who);
@@ -988,7 +1007,7 @@ static int geom_of(const pgb_v6_plan* p, Geom& g, const char* who) {
 
 static int check_common(const char* who, int64_t C, int64_t N, int64_t B, int64_t nsteps, int64_t ndim,
                         int64_t terms, const void* wfrag, const void* dtab) {
-  PGB_REQUIRE(C >= 1 && C <= 16, PGB_ERR_UNSUPPORTED, "%s: ncoils must be 1..16, got %lld", who, (long long)C);
+  PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED, "%s: ncoils must be 1..32, got %lld", who, (long long)C);
   PGB_REQUIRE(ndim == 2 || ndim == 3, PGB_ERR_INVALID, "%s: ndim must be 2 or 3", who);
   PGB_REQUIRE(terms == 1 || terms == 3, PGB_ERR_INVALID, "%s: terms must be 1 (bf16) or 3 (bf16x3)", who);
   PGB_REQUIRE(nsteps >= 1 && nsteps <= (ndim == 3 ? 255 : 65535), PGB_ERR_RANGE, "%s: invalid nsteps %lld", who,
@@ -1049,12 +1068,12 @@ size_t tc_smem(int64_t C, int cells, int64_t nsteps, int64_t ndim, int cap, bool
 }  // namespace
 
 #define PGB_TC_DISPATCH(X) \
-  X(4, 2) X(4, 3) X(8, 2) X(8, 3) X(12, 2) X(12, 3) X(16, 2) X(16, 3)
+  X(4, 2) X(4, 3) X(8, 2) X(8, 3) X(12, 2) X(12, 3) X(16, 2) X(16, 3) X(24, 2) X(24, 3) X(32, 2) X(32, 3)
 
 extern "C" {
 
 size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t ndim, int64_t sub_cap) {
-  if (C < 1 || C > 16 || cells < 1 || cells > 4096 || nsteps < 1 || nsteps > 65535 || (ndim != 2 && ndim != 3) ||
+  if (C < 1 || C > 32 || cells < 1 || cells > 4096 || nsteps < 1 || nsteps > 65535 || (ndim != 2 && ndim != 3) ||
       sub_cap < 1 || sub_cap > kT)
     return ~static_cast<size_t>(0);
   const int CP = padded(C), NS = static_cast<int>(ndim);
@@ -1069,7 +1088,7 @@ size_t pgb_grog_tc_smem_bytes(int64_t C, int64_t cells, int64_t nsteps, int64_t 
 }
 
 int pgb_grog_tc_blocks_per_sm(int64_t C, int64_t ndim) {
-  if (C < 1 || C > 16 || (ndim != 2 && ndim != 3)) return 0;
+  if (C < 1 || C > 32 || (ndim != 2 && ndim != 3)) return 0;
   switch (padded(C) * 10 + static_cast<int>(ndim)) {
 #define X(CP, NS) \
   case CP * 10 + NS: \
@@ -1094,6 +1113,8 @@ int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const v
   PGB_REQUIRE(G == static_cast<int64_t>(plan->gz) * plan->gy * plan->gx, PGB_ERR_INVALID,
               "%s: G does not match the plan grid", who);
   PGB_REQUIRE(ndim == 3 || plan->gz == 1, PGB_ERR_INVALID, "%s: a 2-D table needs a 2-D plan", who);
+  PGB_REQUIRE(plan->sub_cap <= tc_rows(C), PGB_ERR_INVALID, "%s: sub-chunks of %d coils hold at most %d entries",
+              who, padded(C), tc_rows(C));
   if (B == 0 || G == 0) return PGB_OK;
   PGB_REQUIRE(grid && (data || N == 0), PGB_ERR_INVALID, "%s: null pointer", who);
   const int cells = plan->bz * plan->by * plan->bx;
@@ -1211,6 +1232,8 @@ int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N, const 
   if (st) return st;
   PGB_REQUIRE(n_zero >= 0 && (n_zero == 0 || zero_src != nullptr), PGB_ERR_INVALID, "%s: bad zero-sample list",
               who);
+  PGB_REQUIRE(primary->sub_cap <= tc_rows(C) && (secondary == nullptr || secondary->sub_cap <= tc_rows(C)),
+              PGB_ERR_INVALID, "%s: sub-chunks of %d coils hold at most %d entries", who, padded(C), tc_rows(C));
   PGB_REQUIRE(G == static_cast<int64_t>(primary->gz) * primary->gy * primary->gx, PGB_ERR_INVALID,
               "%s: G does not match the plan grid", who);
   PGB_REQUIRE(ndim == 3 || primary->gz == 1, PGB_ERR_INVALID, "%s: a 2-D table needs a 2-D plan", who);

@@ -170,9 +170,17 @@ def test_hot_brick_split_and_repeatability(cuda):
     (3, 24, 300, 48, 12, 1.0, 2, "sphere", 1, 1),  # c1-like kooshball
     (2, 40, 20, 80, 5, 1.5, 3, "cross", 1, 1),     # odd coil count (padded to 8)
     (3, 16, 200, 32, 4, 2.0, 2, "sphere", 1, 1),   # 4 coils, many replicas per cell
+    (3, 16, 200, 32, 32, 2.0, 2, "sphere", 1, 1),  # 32 coils: one m-tile per warp, 128-entry sub-chunks
+    (2, 40, 30, 80, 20, 1.5, 2, "circle", 1, 2),   # 20 coils (padded to 24), batch 2
 ])
 def test_tensor_core_grid_degrid_vs_fp64_oracle(cuda, ndim, n, spokes, readout, C, osf, kwd, ks, prec, B, mode):
-    """bf16x3 ("tc") within 1e-4 of the FP64 oracle; plain bf16 ("tc1") within 2e-2."""
+    """bf16x3 ("tc") within 1e-4 of the FP64 oracle; plain bf16 ("tc1") within 2e-2.
+
+    Above 16 coils the random-noise calibration of these cases gives per-axis
+    eigenvectors with condition numbers up to about 70, which amplify the
+    chain's rounding: there the bounds are 2e-4 and 6e-2 (the smooth-coil
+    32-coil case below holds 1e-4 / 2e-2, and the autotuner measures each
+    tensor-core candidate against its tolerance before installing it)."""
     coords, calib, data = _random_case(ndim, n, spokes, readout, C, osf, kwd, ks, prec, seed=n + C, B=B)
     g = GrogInterpolator(shape=(n,) * ndim, coords=coords, oversamp=osf, kernel_width=kwd,
                          kernel_shape=ks, device=cuda)
@@ -182,7 +190,7 @@ def test_tensor_core_grid_degrid_vs_fp64_oracle(cuda, ndim, n, spokes, readout, 
     p = og.create_plan((n,) * ndim, coords, osf, kwd, ks)
     qi = g._interp_idx.cpu().numpy()
     G = int(np.prod(p["grid_shape"]))
-    tol = 1e-4 if mode == "tc" else 2e-2
+    tol = (1e-4 if mode == "tc" else 2e-2) * (1 if C <= 16 else (2 if mode == "tc" else 3))
     kg = g.grid(data)
     assert g._brick(0).mode == mode
     ref, _ = og.grid(data.reshape(B, C, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
@@ -192,6 +200,50 @@ def test_tensor_core_grid_degrid_vs_fp64_oracle(cuda, ndim, n, spokes, readout, 
     assert rel_l2(out.reshape(B, C, -1), ref_a) < tol
     # repeat: same result (the shared tile / result buffers are re-zeroed)
     assert rel_l2(g.grid(data), kg) < 1e-6
+
+
+def _smooth_calib(C, ndim, n_cal, seed):
+    """Centre ``n_cal``-wide k-space block of C Gaussian-bump coil images of a
+    two-level disc phantom (well-conditioned GRAPPA fits, like measured coils)."""
+    rng = np.random.default_rng(seed)
+    n = 2 * n_cal
+    ax = np.linspace(-1, 1, n)
+    grids = np.meshgrid(*([ax] * ndim), indexing="ij")
+    r2 = sum(a * a for a in grids)
+    ph = (r2 < 0.6).astype(np.float64) + 0.5 * (r2 < 0.2)
+    out = []
+    for _ in range(C):
+        c = rng.uniform(-0.7, 0.7, ndim)
+        img = ph * np.exp(-sum((a - ci) ** 2 for a, ci in zip(grids, c)) / 0.5) * np.exp(1j * rng.uniform(0, 6.28))
+        k = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(img), norm="ortho"))
+        lo = n // 2 - n_cal // 2
+        out.append(k[tuple(slice(lo, lo + n_cal) for _ in range(ndim))])
+    return np.stack(out).astype(np.complex64)
+
+
+@pytest.mark.parametrize("mode", ["tc", "tc1"])
+def test_tensor_core_32_coils_smooth_calibration(cuda, mode):
+    """32 coils (one m-tile per warp, 128-entry sub-chunks, tensor copies of
+    the brick tiles) on a smooth-coil calibration: 1e-4 / 2e-2 of FP64."""
+    C, n = 32, 24
+    coords, _, data = _random_case(3, n, 300, 48, C, 1.0, 2, "sphere", 1, seed=3)
+    calib = _smooth_calib(C, 3, 12, seed=4)
+    g = GrogInterpolator(shape=(n,) * 3, coords=coords, oversamp=1.0, kernel_width=2, kernel_shape="sphere",
+                         device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    g.gridder_mode = mode
+    table = g._interp_kernel.numpy().astype(np.complex128)
+    p = og.create_plan((n,) * 3, coords, 1.0, 2, "sphere")
+    qi = g._interp_idx.cpu().numpy()
+    G = int(np.prod(p["grid_shape"]))
+    tol = 1e-4 if mode == "tc" else 2e-2
+    kg = g.grid(data)
+    assert g._brick(0).mode == mode and g._brick(0).sub_cap == 128
+    ref, _ = og.grid(data.reshape(1, C, -1).astype(np.complex128), qi, table, p, og.fft_plan(p))
+    assert rel_l2(kg.reshape(1, C, G), ref) < tol
+    out = g.degrid(kg)
+    ref_a = og.degrid(np.asarray(kg).reshape(1, C, G).astype(np.complex128), qi, table, p)
+    assert rel_l2(out.reshape(1, C, -1), ref_a) < tol
 
 
 def test_tensor_core_fallback_paths_match(cuda):
@@ -252,6 +304,21 @@ def test_autotuner_picks_a_valid_gridder(cuda):
     clear_cache()
     strict = autotune_gridder(g, tolerance=1e-6, reps=1)
     assert all(t[0] in ("v8", "v6") for t in strict["trials"])
+    # 20 coils: tensor-core families up to 32 coils, the FP32 global gridder beside them
+    clear_cache()
+    coords, calib, data = _random_case(2, 32, 24, 64, 20, 1.0, 2, "circle", 1, seed=5)
+    g = GrogInterpolator(shape=(32, 32), coords=coords, oversamp=1.0, kernel_width=2, device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    res = autotune_gridder(g, tolerance=1e-4, reps=1)
+    assert {t[0] for t in res["trials"]} | {r[0] for r in res["rejected"]} >= {"tc", "global"}
+    assert res["mode"] in ("tc", "global") and all(t[3] <= 1e-4 for t in res["trials"])
+    assert all(r[2] > 1e-4 for r in res["rejected"])
+    p = og.create_plan((32, 32), coords, 1.0, 2, "circle")
+    table = g._interp_kernel.numpy().astype(np.complex128)
+    ref, _ = og.grid(data.reshape(1, 20, -1).astype(np.complex128), g._interp_idx.cpu().numpy(), table, p,
+                     og.fft_plan(p))
+    assert rel_l2(g.grid(data).reshape(1, 20, -1), ref) < 1e-4
+    clear_cache()
 
 
 @pytest.mark.parametrize("case", golden_plan_cases())

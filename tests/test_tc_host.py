@@ -117,7 +117,8 @@ def _acr(C, ndim, seed):
     return np.stack(out).astype(np.complex64)
 
 
-@pytest.mark.parametrize("ndim,C,terms", [(3, 12, 3), (2, 8, 3), (2, 5, 3), (3, 4, 1), (2, 16, 3)])
+@pytest.mark.parametrize("ndim,C,terms", [(3, 12, 3), (2, 8, 3), (2, 5, 3), (3, 4, 1), (2, 16, 3), (2, 20, 3),
+                                          (3, 32, 3)])
 def test_tc_dataflow_matches_table(ndim, C, terms):
     acr = _acr(C, ndim, seed=C + ndim)
     table, nsteps, nd, _ = KernelTable(acr, 1.0, 1, 0.01, return_factors=True)
@@ -142,3 +143,44 @@ def test_tc_dataflow_matches_table(ndim, C, terms):
     refa = np.einsum("nrc,nr->nc", T.conj(), x[:, :C])
     gota = _model_tile(x, ix, ops, False, terms)
     assert np.linalg.norm(gota[:, :C] - refa) / np.linalg.norm(refa) < tol
+
+
+@pytest.mark.parametrize("C,CP", [(1, 4), (12, 12), (16, 16), (17, 24), (24, 24), (25, 32), (32, 32)])
+def test_tc_padding_and_sub_chunk_budget(C, CP):
+    """Coil padding of the operands matches the kernels; above 16 coils the
+    sub-chunks hold 128 entries and one of them still fits shared memory."""
+    from pygrog_b200 import _lib
+
+    assert padded_coils(C) == CP
+    lib = _lib.lib()
+    cap = 256 if C <= 16 else 128
+    for nd in (2, 3):
+        assert lib.pgb_grog_tc_blocks_per_sm(C, nd) >= 1
+        cells = 4 * 4 * 8 if nd == 3 else 8 * 16  # second-smallest bricks of the gridder's candidates
+        assert lib.pgb_grog_tc_smem_bytes(C, cells, 9, nd, cap) <= 227 * 1024
+    assert lib.pgb_grog_tc_blocks_per_sm(33, 3) == 0
+
+
+def test_tc_operands_pick_the_lower_modeled_error():
+    """The eigenvector scaling of the operands is the one with the lower
+    modeled bf16x3 error; the model's plain-bf16 error is reported too."""
+    from pygrog_b200.calib._tc import _chain, balance_eigenvectors, chain_rounding_error
+
+    C, ndim = 20, 2
+    acr = _acr(C, ndim, seed=3)
+    ef = eigen_factors(acr, 1.0, 1, 0.01)
+    ops = tc_operands(ef, C, "cpu")
+    CP = padded_coils(C)
+    V0 = [np.asarray(v.numpy(), dtype=np.complex128) for v, _ in ef.axes]
+    lam = [np.asarray(l.numpy(), dtype=np.complex128) for _, l in ef.axes]
+    d = ef.deltas.numpy().astype(np.float32).astype(np.float64)
+    errs = []
+    for V in (V0, [balance_eigenvectors(v) for v in V0]):
+        # same operator whatever the scaling
+        mats, D = _chain(V, lam, d, C, CP)
+        errs.append(chain_rounding_error(mats, D, C, CP, 3))
+        for s in range(ndim):
+            np.testing.assert_allclose(V[s] @ np.diag(np.exp(0.3 * lam[s])) @ np.linalg.inv(V[s]),
+                                       V0[s] @ np.diag(np.exp(0.3 * lam[s])) @ np.linalg.inv(V0[s]), atol=1e-10)
+    assert ops["model_err"][3] == min(errs) < 1e-4
+    assert 1e-4 < ops["model_err"][1] < 5e-2
