@@ -529,7 +529,7 @@ def cg_sense_c2(dev, iters: int = 30) -> dict:
 
 
 def main():
-    global N_SPOKES, N_READOUT, GRID_N
+    global N_SPOKES, N_READOUT, GRID_N, N_COILS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
@@ -546,11 +546,14 @@ def main():
     ap.add_argument("--spokes", type=int, default=N_SPOKES, help="smaller cases for profiling only")
     ap.add_argument("--readout", type=int, default=N_READOUT)
     ap.add_argument("--grid", type=int, default=GRID_N)
+    ap.add_argument("--coils", type=int, default=N_COILS, help=f"virtual coils after PCA of {N_COILS_RAW} (1..32)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="open-loop serving duration (0: skip)")
     ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
     args = ap.parse_args()
-    resized = (args.spokes, args.readout, args.grid) != (N_SPOKES, N_READOUT, GRID_N)
-    N_SPOKES, N_READOUT, GRID_N = args.spokes, args.readout, args.grid
+    resized = (args.spokes, args.readout, args.grid, args.coils) != (N_SPOKES, N_READOUT, GRID_N, N_COILS)
+    if not 1 <= args.coils <= N_COILS_RAW:
+        ap.error(f"--coils must be 1..{N_COILS_RAW}")
+    N_SPOKES, N_READOUT, GRID_N, N_COILS = args.spokes, args.readout, args.grid, args.coils
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":
@@ -624,7 +627,8 @@ def main():
     dom_ms = max(fwd_ms, adj_ms)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
-    traffic, tsrc = _profile_traffic(dom)
+    # DRAM traffic per launch from the committed launch-list profile of the default workload
+    traffic, tsrc = _profile_traffic(dom) if not resized else (None, None)
     n_launch = bp.launches_per_call(False) + bp.launches_per_call(True)
 
     # end to end through the public API with host buffers (pinned)
@@ -661,7 +665,8 @@ def main():
     modes = None
     if ws == 1 and not args.no_precision_modes:
         try:
-            modes = time_modes(g, data, [m for m in ("v8", "tc", "tc1") if m != "auto"], ref_fwd, chk)
+            fp32 = "v8" if N_COILS <= 16 else "global"  # the shared-memory FP32 families stop at 16 coils
+            modes = time_modes(g, data, [fp32, "tc", "tc1"], ref_fwd, chk)
         except Exception as exc:  # noqa: BLE001
             modes = {"error": f"{type(exc).__name__}: {exc}"}
     del ref_fwd, chk
@@ -672,7 +677,8 @@ def main():
 
         saved_mode = getattr(g, "gridder_mode", None)
         tune = autotune_gridder(g, batch=B, tolerance=1e-4, reps=3)
-        tune["trials"] = [[m, list(b), t] for m, b, t in tune["trials"]]
+        tune["trials"] = [[m, list(b), t, e] for m, b, t, e in tune["trials"]]
+        tune["rejected"] = [[m, list(b), e] for m, b, e in tune["rejected"]]
         tune["brick"] = list(tune["brick"])
         g.gridder_mode, g.gridder_brick, g._brick_plans = saved_mode, None, None
         torch.cuda.empty_cache()
@@ -707,7 +713,7 @@ def main():
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
                        "sample": f"failed: {exc}"}
         line = {
-            "metric": METRIC,
+            "metric": METRIC if not resized else METRIC.replace("192^3, C=12", f"{GRID_N}^3, C={N_COILS}"),
             "value": value,
             "unit": UNIT,
             "n_gpus": ws,
@@ -723,11 +729,11 @@ def main():
             "precision_modes": modes,
             "autotune": tune,
             "config": {
-                "workload": (f"grog3d_kooshball_{GRID_N}c12_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
+                "workload": (f"grog3d_kooshball_{GRID_N}c{N_COILS}_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
                              else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode + ("/pairs" if getattr(bp, "pairs", False) else ""), "kernels": list(bp.kernel_names()), "l2": "inputs larger than L2 (737 MB samples, 679 MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode + ("/pairs" if getattr(bp, "pairs", False) else ""), "kernels": list(bp.kernel_names()), "l2": f"inputs larger than L2 ({N * C * 8 / 1e6:.0f} MB samples, {G * C * 8 / 1e6:.0f} MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
             "fwd_ms": fwd_ms,
