@@ -528,6 +528,74 @@ def cg_sense_c2(dev, iters: int = 30) -> dict:
             "note": "recon = GROG interpolate + SparseFFT adjoint + graph-replayed CG (Toeplitz normal)"}
 
 
+def _call_workloads():
+    """(name, Workload, CG damp) of the per-call timings: configs c0 and c2."""
+    from pygrog_b200.workloads import config0, config2
+
+    return [("c0", config0(), 1e-2), ("c2", config2(), 1e-3)]
+
+
+def time_calls(dev, reps: int = 5) -> dict:
+    """Per-call device times of the public API on configs c0 and c2, inputs
+    resident on the GPU: plan, table fit (host FP64 and device), interpolate,
+    interpolate(grid=True), degrid, SparseFFT build (Toeplitz PSF), forward,
+    adjoint, normal, solve(cg, 30).  One warm-up, then ``reps`` repeats, each
+    bracketed by a synchronize; median and min in ms."""
+    import torch
+
+    from pygrog_b200.calib import GrogInterpolator
+    from pygrog_b200.operator import SparseFFT
+
+    def timed(fn, setup=None):
+        """``fn(setup())`` after one warm-up; ``setup`` runs outside the timed region."""
+        fn(setup()) if setup else fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(reps):
+            arg = setup() if setup else None
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            fn(arg) if setup else fn()
+            torch.cuda.synchronize(dev)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return {"median_ms": float(np.median(ts)), "min_ms": float(np.min(ts))}
+
+    out = {}
+    for name, w, damp in _call_workloads():
+        res = {}
+        mk = lambda: GrogInterpolator(shape=w.shape, coords=w.coords, oversamp=w.oversamp,  # noqa: E731
+                                      kernel_width=w.kernel_width, kernel_shape=w.kernel_shape, device=dev)
+        res["plan"] = timed(mk)
+        res["calc_interp_table"] = timed(
+            lambda gi: gi.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision), setup=mk)
+        res["calc_interp_table_device_fit"] = timed(
+            lambda gi: gi.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision, fit_on_device=True),
+            setup=mk)
+        g = mk()
+        g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)
+        data = torch.from_numpy(w.data).to(dev)
+        res["interpolate"] = timed(lambda: g.interpolate(data))
+        res["interpolate_grid"] = timed(lambda: g.interpolate(data, grid=True))
+        kg = g.grid(data)
+        res["degrid"] = timed(lambda: g.degrid(kg))
+        smaps = torch.from_numpy(w.smaps.astype(np.complex64)).to(dev)
+        res["sparsefft_build_toeplitz"] = timed(lambda: SparseFFT(plan=g.plan, smaps=smaps, toeplitz=True))
+        op = SparseFFT(plan=g.plan, smaps=smaps, toeplitz=True)
+        sparse = torch.as_tensor(g.interpolate(data))
+        b = sparse * g.plan.pre_weights.unsqueeze(0)
+        x = op.adjoint(b)
+        res["forward"] = timed(lambda: op.forward(x))
+        res["adjoint"] = timed(lambda: op.adjoint(b))
+        res["normal"] = timed(lambda: op.normal(x))
+        bn = b.reshape(b.shape[0], *op.natural_shape)
+        res["solve_cg30"] = timed(lambda: op.solve(bn, method="cg", max_iter=30, damp=damp, tol=0.0))
+        out[name] = {"shape": list(w.shape), "coils": int(w.data.shape[0]), "samples": int(np.prod(w.data.shape[1:])),
+                     "calls": res}
+        del g, op
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     global N_SPOKES, N_READOUT, GRID_N, N_COILS
     ap = argparse.ArgumentParser()
@@ -549,6 +617,8 @@ def main():
     ap.add_argument("--coils", type=int, default=N_COILS, help=f"virtual coils after PCA of {N_COILS_RAW} (1..32)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="open-loop serving duration (0: skip)")
     ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
+    ap.add_argument("--calls", action="store_true",
+                    help="only time the public API call by call on configs c0 and c2 (one JSON line)")
     args = ap.parse_args()
     resized = (args.spokes, args.readout, args.grid, args.coils) != (N_SPOKES, N_READOUT, GRID_N, N_COILS)
     if not 1 <= args.coils <= N_COILS_RAW:
@@ -572,6 +642,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.calls:
+        if rank == 0:
+            print(json.dumps({"calls": time_calls(dev), "device": torch.cuda.get_device_name(dev),
+                              "inputs": "device-resident", "timing": "synchronize around each call"}), flush=True)
+        return 0
 
     g, coords, acr, data = build_workload(dev)
     if args.table_mode and args.table_mode != "auto":

@@ -18,6 +18,8 @@ from __future__ import annotations
 
 __all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG", "BatchedDeviceCG"]
 
+import gc
+import weakref
 from collections.abc import Callable
 from typing import Any
 
@@ -45,8 +47,10 @@ def _vdot_re64(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
 class DeviceCG:
     """CG state for one frame on the device (FP64 scalars, optional CUDA graph)."""
 
-    def __init__(self, op, AHb: torch.Tensor, damp: float, tol: float, x0=None):
-        self.op = op
+    def __init__(self, op, AHb: torch.Tensor, damp: float, tol: float, x0=None, weak_op: bool = False):
+        # a solver cached on its operator refers to it weakly: no reference cycle whose
+        # collection (at any time, e.g. inside another graph capture) would free a graph
+        self.op = weakref.proxy(op) if weak_op else op
         dev = AHb.device
         self.damp = float(damp)
         self.x = torch.zeros_like(AHb) if x0 is None else x0.to(dev, torch.complex64).clone()
@@ -63,10 +67,26 @@ class DeviceCG:
         self.scratch = torch.zeros((nbytes + 7) // 8, dtype=torch.float64, device=dev)
         self.scal = torch.zeros(8, dtype=torch.float64, device=dev)
         self.scal[6] = float(tol)
+        self.tol = float(tol)
         st = _lib.stream_ptr(dev)
         _lib.call("pgb_dot_f64", self.r.data_ptr(), None, self.n, self.scratch.data_ptr(),
                   self.scal.data_ptr(), 0, 2, st)
         self.graph = None
+
+    def reset(self, AHb: torch.Tensor, x0=None):
+        """Start a new solve in the same buffers (a captured iteration graph stays valid)."""
+        if x0 is None:
+            self.x.zero_()
+            self.r.copy_(AHb)
+        else:
+            self.x.copy_(x0)
+            self.op._normal_into(self.x, self.Ap, self.damp)
+            torch.sub(AHb, self.Ap, out=self.r)
+        self.p.copy_(self.r)
+        self.scal.zero_()
+        self.scal[6] = self.tol
+        _lib.call("pgb_dot_f64", self.r.data_ptr(), None, self.n, self.scratch.data_ptr(),
+                  self.scal.data_ptr(), 0, 2, _lib.stream_ptr(self.p.device))
 
     def step(self):
         st = _lib.stream_ptr(self.p.device)
@@ -91,13 +111,20 @@ class DeviceCG:
         for t, v in zip((self.x, self.r, self.p, self.scal), saved):
             t.copy_(v)
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self.step()
+        gc_on = gc.isenabled()
+        gc.disable()  # no collection (and no CUDA frees it may trigger) while capturing
+        try:
+            with torch.cuda.graph(g):
+                self.step()
+        finally:
+            if gc_on:
+                gc.enable()
         self.graph = g
 
     def run(self, max_iter: int, callback: Callable | None = None, use_graph: bool = True):
         if callback is None and use_graph and max_iter > 1:
-            self.capture()
+            if self.graph is None:
+                self.capture()
             for _ in range(max_iter):
                 self.graph.replay()
             return self.x
@@ -176,9 +203,15 @@ class BatchedDeviceCG:
         if self._pool is None:
             self._pool = torch.cuda.graph_pool_handle()
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, pool=self._pool):
-            for _ in range(int(max_iter)):
-                self.step()
+        gc_on = gc.isenabled()
+        gc.disable()  # no collection (and no CUDA frees it may trigger) while capturing
+        try:
+            with torch.cuda.graph(g, pool=self._pool):
+                for _ in range(int(max_iter)):
+                    self.step()
+        finally:
+            if gc_on:
+                gc.enable()
         self._graphs[(int(frames), int(max_iter))] = g
 
     def run(self, max_iter: int) -> torch.Tensor:
@@ -204,6 +237,32 @@ def _device_cg_applicable(op, AHb, preconditioner) -> bool:
     )
 
 
+_CG_GRAPHS_PER_OP = 4
+
+
+def _cached_solver(op, AHb: torch.Tensor, damp: float, tol: float, x0d) -> DeviceCG:
+    """Graph-replayed CG solver of ``op`` for this right-hand side shape, damp
+    and tolerance, kept on the operator so that repeated solves replay the
+    captured iteration instead of capturing it again (the key includes the
+    coil maps' buffer, the state the captured normal operator reads)."""
+    smaps = getattr(op, "_smaps_d", None)
+    key = (tuple(AHb.shape), str(AHb.device), float(damp), float(tol), bool(getattr(op, "toeplitz", False)),
+           smaps.data_ptr() if isinstance(smaps, torch.Tensor) else 0)
+    cache = getattr(op, "_cg_graphs", None)
+    if cache is None:
+        cache = {}
+        op._cg_graphs = cache
+    solver = cache.pop(key, None)
+    if solver is None:
+        solver = DeviceCG(op, AHb, damp, tol, x0d, weak_op=True)
+        while len(cache) >= _CG_GRAPHS_PER_OP:
+            cache.pop(next(iter(cache)))
+    else:
+        solver.reset(AHb, x0d)
+    cache[key] = solver  # most recently used last
+    return solver
+
+
 def cg(
     op: Any,
     b: torch.Tensor,
@@ -223,7 +282,10 @@ def cg(
         b = b.to(op._cdev)
     AHb = op.adjoint(b)
     if _device_cg_applicable(op, AHb, preconditioner):
-        x0d = None if x0 is None else torch.as_tensor(x0).to(AHb.device)
+        x0d = None if x0 is None else torch.as_tensor(x0).to(AHb.device, torch.complex64)
+        if use_graph and callback is None and int(max_iter) > 1:
+            solver = _cached_solver(op, AHb, damp, tol, x0d)
+            return solver.run(int(max_iter), None, True).clone().to(src_dev)
         solver = DeviceCG(op, AHb, damp, tol, x0d)
         x = solver.run(int(max_iter), callback, use_graph)
         return x.to(src_dev)

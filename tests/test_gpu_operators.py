@@ -93,6 +93,29 @@ def test_cg_early_exit_matches_break(cuda):
     assert rel_l2(x_gr.numpy(), x_cb.numpy()) < 1e-6
 
 
+def test_repeated_solves_replay_the_cached_graph(cuda):
+    """Solves on one operator reuse its captured CG iteration: each result
+    equals a fresh host-loop solve, earlier results are not overwritten, and
+    a warm start (x0) and another damp take their own paths."""
+    z, g, C = _plan("op2d", cuda)
+    sm = torch.from_numpy(z["in_smaps"])
+    op = SparseFFT(plan=g.plan, smaps=sm, toeplitz=True)
+    bn = torch.from_numpy(z["in_b"]).reshape(C, *op.natural_shape)
+    x1 = op.solve(bn, method="cg", max_iter=8, damp=1e-3, tol=0.0)
+    b2 = bn * 0.5 + 0.25j * torch.roll(bn, 3, dims=-1)
+    x2 = op.solve(b2, method="cg", max_iter=8, damp=1e-3, tol=0.0)
+    assert len(op._cg_graphs) == 1
+    assert rel_l2(x1.numpy(), z["ref_cg"]) < 1e-4  # x1 kept its values
+    ref2 = op.solve(b2, method="cg", max_iter=8, damp=1e-3, tol=0.0, use_graph=False)
+    assert rel_l2(x2.numpy(), ref2.numpy()) < 1e-6
+    x3 = op.solve(b2, method="cg", max_iter=8, damp=1e-2, tol=0.0)
+    assert len(op._cg_graphs) == 2
+    assert rel_l2(x3.numpy(), op.solve(b2, method="cg", max_iter=8, damp=1e-2, tol=0.0, use_graph=False).numpy()) < 1e-6
+    x4 = op.solve(b2, method="cg", max_iter=8, damp=1e-3, tol=0.0, x0=x1)
+    ref4 = op.solve(b2, method="cg", max_iter=8, damp=1e-3, tol=0.0, x0=x1, use_graph=False)
+    assert rel_l2(x4.numpy(), ref4.numpy()) < 1e-6
+
+
 @pytest.mark.parametrize("name", ["op2d", "op3d"])
 def test_masked_fft_matches_reference(cuda, name):
     z, g, C = _plan(name, cuda)
