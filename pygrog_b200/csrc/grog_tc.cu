@@ -55,6 +55,10 @@ namespace tc {
 constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk (128 above 16 coils)
 constexpr int kFirst = 1, kLast = 2, kSplit = 4;
 
+// 16-byte groups of B-fragment words per n-tile (head or tail) for CP coils:
+// ceil((2 * k16 chunks + k8 chunk) / 4), k16 = CP / 8, k8 = (CP / 4) % 2
+__host__ __device__ constexpr int tc_wq(int CP) { return (2 * (CP / 8) + (CP / 4) % 2 + 3) / 4; }
+
 template <int CP>
 struct Shape {
   static constexpr int NT = CP / 4;                   // n-tiles of 8 real columns (4 complex coils)
@@ -63,6 +67,7 @@ struct Shape {
   static constexpr int NFR = NT * (2 * K16 + K8);     // B-fragment words per lane per matrix
   static constexpr int FPN = 2 * K16 + K8;            // words per n-tile
   static constexpr int WQ = (FPN + 3) / 4;            // 16-byte groups per n-tile and head / tail
+  static_assert(WQ == tc_wq(CP), "fragment group count");
   static constexpr int TS = CP + 1;                   // tile stride per cell (float2): conflict-free flush
   // m-tiles a warp runs side by side: two up to 16 coils (256-entry
   // sub-chunks), one above (128-entry sub-chunks: the registers of one tile)
@@ -460,8 +465,7 @@ struct Smem {
     dt = 0;
     const Phases ph(CP, NS, nsteps);
     wf = (ph.copies * ph.copy_sz + 1) & ~1;       // W fragments: (NS + 1) * (CP / 4) * 2 * WQ * 32 uint4
-    const int wq = ((2 * (CP / 8) + (CP / 4) % 2) + 3) / 4;  // Shape<CP>::WQ
-    tile = wf + (NS + 1) * (CP / 4) * 2 * wq * 32 * 2;  // float2 units
+    tile = wf + (NS + 1) * (CP / 4) * 2 * tc_wq(CP) * 32 * 2;  // float2 units
     if (tma) {
       tile = (tile + 15) & ~15;  // 128-byte aligned TMA boxes, [coil][cell]
       tile_sz = (cells * CP + 15) & ~15;
