@@ -329,7 +329,8 @@ def coil_compress_c1(dev, reps: int = 5) -> dict:
             "fp32": {"kernel": "coil_compress_kernel<32>", "ms": ms, "achieved_gbs": gbs, "roofline_frac": gbs / peak},
             "bf16x3": {"kernel": "coil_compress_tc_kernel<32,2>", "ms": ms_tc, "achieved_gbs": gbs_tc,
                        "roofline_frac": gbs_tc / peak, "rel_err_vs_fp32_kernel": err_tc},
-            "peak_source": kind, "fit_s_incl_fp64_covariance": fit_s}
+            "peak_source": kind, "fit_s_incl_fp64_covariance": fit_s,
+            "tc_ms": ms_tc, "tc_gbs": gbs_tc, "tc_frac": gbs_tc / peak, "fp32_ms": ms, "tc_rel_err_vs_fp32": err_tc}
 
 
 def cpu_baseline(coords, acr, spokes: int):
@@ -596,6 +597,45 @@ def time_calls(dev, reps: int = 5) -> dict:
     return out
 
 
+def _r(v, nd=4):
+    """Round floats for the one-line summary (None and non-floats pass)."""
+    return float(f"{v:.{nd}g}") if isinstance(v, float) else v
+
+
+def _compact_modes(modes):
+    """{mode: [fwd_ms, adj_ms, rel_err_fwd, rel_err_adj]} of the precision comparison."""
+    if not isinstance(modes, dict) or "error" in modes:
+        return modes
+    return {m: [_r(v["fwd_ms"]), _r(v["adj_ms"]), _r(v["rel_err_fwd_vs_fp64"], 2), _r(v["rel_err_adj_vs_fp64"], 2)]
+            for m, v in modes.items()}
+
+
+def _compact_sections(coilc, cg2, c3, serving, tune):
+    """Headline numbers of the secondary sections, short enough for one line."""
+    out = {}
+
+    def pick(d, keys):
+        if not isinstance(d, dict):
+            return d
+        if "error" in d:
+            return {"error": str(d["error"])[:160]}
+        return {k: _r(d[k]) for k in keys if k in d}
+
+    out["coil_compress_c1"] = pick(coilc, ("tc_ms", "tc_gbs", "tc_frac", "fp32_ms", "tc_rel_err_vs_fp32"))
+    out["cg_sense_c2"] = pick(cg2, ("ms_per_recon", "ms_per_iter", "iter_roofline_frac"))
+    out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "sample_coils_per_s", "setup_s", "mode"))
+    if isinstance(serving, dict) and "error" not in serving:
+        o = serving.get("open_loop", {})
+        out["serving"] = {k: _r(serving.get(k)) for k in ("closed_loop_recons_per_s", "single_instance_recons_per_s",
+                                                         "batched_over_single")}
+        out["serving"].update({k: _r(o.get(k)) for k in ("rate_per_s", "p50_ms", "p95_ms", "p99_ms", "mean_batch")})
+    else:
+        out["serving"] = pick(serving, ())
+    if tune:
+        out["autotune"] = {"mode": tune.get("mode"), "brick": tune.get("brick"), "ms": _r(tune.get("ms"))}
+    return out
+
+
 def main():
     global N_SPOKES, N_READOUT, GRID_N, N_COILS
     ap = argparse.ArgumentParser()
@@ -619,6 +659,8 @@ def main():
     ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
     ap.add_argument("--calls", action="store_true",
                     help="only time the public API call by call on configs c0 and c2 (one JSON line)")
+    ap.add_argument("--details", default=None,
+                    help="also write the full per-section results (precision modes, serving, c2, c3) to this file")
     args = ap.parse_args()
     resized = (args.spokes, args.readout, args.grid, args.coils) != (N_SPOKES, N_READOUT, GRID_N, N_COILS)
     if not 1 <= args.coils <= N_COILS_RAW:
@@ -787,6 +829,10 @@ def main():
             except Exception as exc:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
                        "sample": f"failed: {exc}"}
+        details = {"precision_modes": modes, "autotune": tune, "coil_compress_c1": coilc, "cg_sense_c2": cg2,
+                   "c3_batch": c3, "serving": serving}
+        if args.details:
+            pathlib.Path(args.details).write_text(json.dumps(details, indent=1))
         line = {
             "metric": METRIC if not resized else METRIC.replace("192^3, C=12", f"{GRID_N}^3, C={N_COILS}"),
             "value": value,
@@ -801,8 +847,7 @@ def main():
             "dtype": {"tc": "bf16x3 (fp32 accumulate)", "tc1": "bf16 (fp32 accumulate)"}.get(bp.mode, "fp32"),
             "data": "synthetic",
             "accuracy": accuracy,
-            "precision_modes": modes,
-            "autotune": tune,
+            "precision_modes": _compact_modes(modes),
             "config": {
                 "workload": (f"grog3d_kooshball_{GRID_N}c{N_COILS}_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
                              else "grog3d_kooshball_192c12_fwd_adj"),
@@ -823,10 +868,7 @@ def main():
             "gpu_launches": n_launch * args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "coil_compress_c1": coilc,
-            "cg_sense_c2": cg2,
-            "c3_batch": c3,
-            "serving": serving,
+            "summary": _compact_sections(coilc, cg2, c3, serving, tune),
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -370,10 +370,19 @@ PGB_API int pgb_grog_degrid_tc(const void* grid, int64_t G, void* out, int64_t N
  * (negative: query only) and returns the previous setting.  No reference
  * counterpart (performance switch). */
 PGB_API int pgb_grog_tc_use_tma(int64_t enable);
-/* Number of tile waits that gave up (bounded mbarrier spin; the kernel then
- * returns without writing that brick's results); reset when reset != 0.
- * Synchronous.  No reference counterpart (diagnostics). */
+/* Number of tile waits that gave up (bounded mbarrier spin; the CTA then
+ * lets its copies in flight land and returns without writing the rest of its
+ * results); reset when reset != 0.  Synchronous.  The Python layer raises
+ * RuntimeError when it reads a non-zero count.  No reference counterpart
+ * (diagnostics). */
 PGB_API int pgb_grog_tc_timeouts(int64_t* count, int64_t reset);
+/* Spin limit of the adjoint's tile waits for later launches (limit >= 0;
+ * -1 restores the default of 2^26 polls); the previous limit goes to
+ * *previous when it is non-null.  Synchronous.  A limit of 0 makes every
+ * tile wait give up at once, which exercises the timeout path without any
+ * fault: the copies still complete and are drained before the CTA exits.
+ * No reference counterpart (failure-path testing). */
+PGB_API int pgb_grog_tc_wait_limit(int64_t limit, int64_t* previous);
 
 /* =====================================================================
  * Coil compression (the step before the path)
@@ -505,6 +514,44 @@ PGB_API int pgb_cg_update_p_batched(void* p, const void* r, int64_t n, int64_t f
 PGB_API int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream);
 
 /* =====================================================================
+ * LSMR with device-resident FP64 scalars.
+ * replaces: _solve/_solvers.py:145-262 (lsmr: Golub-Kahan step, rotations
+ * Q_k / Qbar_k, h / hbar / x updates, stopping test |zetabar| / |b| <
+ * atol + btol), whose norms are FP32 and whose branches and stopping test
+ * are host .item() reads.
+ *
+ * Scalar block: double[PGB_LSMR_SCALARS] in device memory, slots
+ *   0 alpha  1 beta  2 alphabar  3 rho  4 rhobar  5 cbar  6 sbar  7 zetabar
+ *   8 zeta  9 normb  10 stop  11 tol (atol + btol)  12 damp  13-15 the
+ *   hbar / x / h update coefficients  16 |u|^2  17 |v_full|^2  18 ran
+ *   19 rel  20 v updated  21 iterations.
+ * The caller initialises slots 0-12 (Fong & Saunders' start: alpha, beta =
+ * |b|, alphabar = alpha, rho = rhobar = cbar = 1, sbar = 0, zetabar =
+ * alpha beta, normb = beta, stop = 0) and runs per iteration, on one stream:
+ *   Av = A v;  pgb_lsmr_u_update(u, Av);  pgb_lsmr_u_scale(u);
+ *   Atu = A^H u;  pgb_lsmr_v_full(vf, Atu, v);  pgb_lsmr_scalars;
+ *   pgb_lsmr_vec_update(x, h, hbar, v, vf).
+ * Norms accumulate in FP64; vectors are complex64.  Once the stopping test
+ * has fired every later call leaves vectors and scalars unchanged, so a
+ * captured iteration can be replayed max_iter times.  scratch holds
+ * pgb_lsmr_scratch_bytes() bytes, zero-initialised once; calls that share a
+ * scratch must be ordered on one stream. */
+#define PGB_LSMR_SCALARS 32
+PGB_API size_t pgb_lsmr_scratch_bytes(void);
+/* u <- Av - alpha u ; slot 16 <- |u|^2 */
+PGB_API int pgb_lsmr_u_update(void* u, const void* Av, int64_t n, void* scal, void* scratch, void* stream);
+/* u <- u / sqrt(slot 16) when slot 16 > 0 */
+PGB_API int pgb_lsmr_u_scale(void* u, int64_t n, const void* scal, void* stream);
+/* vf <- Atu - beta v (beta = sqrt(slot 16)) ; slot 17 <- |vf|^2 ; only when slot 16 > 0 */
+PGB_API int pgb_lsmr_v_full(void* vf, const void* Atu, const void* v, int64_t n, void* scal, void* scratch,
+                            void* stream);
+/* the scalar recurrence of one iteration (one thread) */
+PGB_API int pgb_lsmr_scalars(void* scal, void* stream);
+/* v <- vf / alpha (when updated) ; hbar <- h - c1 hbar ; x <- x + c2 hbar ; h <- v - c3 h */
+PGB_API int pgb_lsmr_vec_update(void* x, void* h, void* hbar, void* v, const void* vf, int64_t n,
+                                const void* scal, void* stream);
+
+/* =====================================================================
  * Allocation-free row inner products.  No counterpart in the reference
  * (FiRMLAB-Pisa/pygrog has no C entry point of this kind; its solvers call
  * torch.vdot, _solve/_solvers.py:49-139).
@@ -524,8 +571,10 @@ PGB_API int pgb_axpy(void* y, const void* x, float a, int64_t n, void* stream);
  *
  * Limit: rows <= 64; larger rows return PGB_ERR_RANGE with a message.
  * The first call on each device looks up the scratch address (with that
- * device current) and caches it; make that first call before any stream
- * capture.  Every call clears the counters it uses on `stream` before its
+ * device current) and caches it together with the current context; a call
+ * that finds another context current (after cudaDeviceReset, say) looks the
+ * address up again.  Make the first call on a device, and the first one
+ * after a reset, before any stream capture.  Every call clears the counters it uses on `stream` before its
  * kernel runs.  All calls on one device share the one scratch array, so
  * calls that can overlap on the GPU (different streams without ordering
  * between them) race and give wrong results: order them on one stream. */

@@ -10,19 +10,33 @@ References (FiRMLAB-Pisa/pygrog):
   Toeplitz normal             _toep/_grog_toep.py:154-209
   MaskedFFT                   operator/_masked_fft.py:322-430
   CG                          _solve/_solvers.py:49-139
+  LSMR                        _solve/_solvers.py:145-262
 """
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 
+try:  # the same pocketfft algorithm, multi-threaded (large FP64 CG-SENSE checks)
+    import scipy.fft as _fft
+
+    _FFT_KW = {"workers": os.cpu_count() or 1}
+except ImportError:  # pragma: no cover
+    _fft = np.fft
+    _FFT_KW = {}
+
+
 def fftc(x, axes):
-    return np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho"), axes=axes)
+    return np.fft.fftshift(_fft.fftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho", **_FFT_KW),
+                           axes=axes)
 
 
 def ifftc(x, axes):
-    return np.fft.fftshift(np.fft.ifftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho"), axes=axes)
+    return np.fft.fftshift(_fft.ifftn(np.fft.ifftshift(x, axes=axes), axes=axes, norm="ortho", **_FFT_KW),
+                           axes=axes)
 
 
 def _slices(grid_shape, image_shape):
@@ -109,6 +123,53 @@ def cg(normal, AHb, damp=0.0, max_iter=20, tol=0.0):
         rz_new = np.vdot(r, r).real
         p = r + rz_new / (rz + 1e-30) * p
         rz = rz_new
+    return x
+
+
+def lsmr(forward, adjoint, b, damp=0.0, max_iter=20, atol=1e-6, btol=1e-6):
+    """_solvers.py:145-262 in complex128 / FP64 scalars (x0 = 0)."""
+    beta = np.linalg.norm(b)
+    if beta == 0:
+        return adjoint(b)
+    u = b / beta
+    v = adjoint(u)
+    alpha = np.linalg.norm(v)
+    if alpha == 0:
+        return np.zeros_like(v)
+    v = v / alpha
+    zetabar, alphabar = alpha * beta, alpha
+    rho = rhobar = cbar = 1.0
+    sbar = 0.0
+    h, hbar = v.copy(), np.zeros_like(v)
+    x = np.zeros_like(v)
+    normb = beta
+    for _ in range(max_iter):
+        u = forward(v) - alpha * u
+        beta = np.linalg.norm(u)
+        if beta > 0:
+            u = u / beta
+            vf = adjoint(u) - beta * v
+            alpha = np.linalg.norm(vf)
+            if alpha > 0:
+                v = vf / alpha
+        alphahat = np.sqrt(alphabar**2 + damp**2)
+        rhoold = rho
+        rho = np.sqrt(alphahat**2 + beta**2)
+        c, s = alphahat / rho, beta / rho
+        thetanew = s * alpha
+        alphabar = c * alpha
+        rhobarold = rhobar
+        thetabar = sbar * rho
+        rhotemp = cbar * rho
+        rhobar = np.sqrt(rhotemp**2 + thetanew**2)
+        cbar, sbar = rhotemp / rhobar, thetanew / rhobar
+        zeta = cbar * zetabar
+        zetabar = -sbar * zetabar
+        hbar = h - (thetabar * rho / (rhoold * rhobarold)) * hbar
+        x = x + (zeta / (rho * rhobar)) * hbar
+        h = v - (thetanew / rho) * h
+        if abs(zetabar) / (normb + 1e-30) < atol + btol:
+            break
     return x
 
 

@@ -65,19 +65,32 @@ class ReferenceCPU:
         self.t_inv = t.from_numpy(self.fplan["inv_perm"])
         self.t_prew = self.t_sqw[self.t_inv]
 
+    def _interpolate(self, data: np.ndarray):
+        """calib/_grog.py:668-695: replicate every sample kw times, shift each
+        replica by its table entry (``grog_interpolate``), back to (C, N kw)."""
+        t = self.torch
+        C, N = data.shape
+        kw = self.kw
+        x = t.from_numpy(np.ascontiguousarray(data))
+        rep = x.unsqueeze(-1).expand(-1, -1, kw).reshape(C, N * kw)
+        di = rep.T.reshape(N * kw, 1, C).contiguous()
+        res = self.ext.grog_interpolate(di, self.t_idx, self.t_tab)
+        di.copy_(res)
+        return di.permute(1, 2, 0).contiguous().reshape(C, N * kw)
+
+    def interpolate(self, data: np.ndarray) -> np.ndarray:
+        """data (C, N) complex64 -> shifted replicas (C, N kw) (``interpolate(data)``)."""
+        if self.ext is None:
+            return og.interpolate(data[None], self.interp_idx.reshape(self.N, -1), self.table)[0]
+        return self._interpolate(data).numpy()
+
     def forward(self, data: np.ndarray) -> np.ndarray:
         """data (C, N) complex64 -> kgrid (C, G)."""
         if self.ext is None:
             return og.grid(data[None], self.interp_idx, self.table, self.plan, self.fplan)[0][0]
         t = self.torch
         C, N = data.shape
-        kw = self.kw
-        x = t.from_numpy(data)
-        rep = x.unsqueeze(-1).expand(-1, -1, kw).reshape(C, N * kw)
-        di = rep.T.reshape(N * kw, 1, C).contiguous()
-        res = self.ext.grog_interpolate(di, self.t_idx, self.t_tab)
-        di.copy_(res)
-        sparse = di.permute(1, 2, 0).contiguous().reshape(C, N * kw)
+        sparse = self._interpolate(data)
         sdc = sparse * self.t_prew.to(sparse.dtype)
         grid = t.zeros(C, self.G, dtype=sparse.dtype)
         for c in range(C):

@@ -142,6 +142,12 @@ _SIGS = {
     "pgb_grog_tc_blocks_per_sm": [_i64, _i64],
     "pgb_grog_tc_use_tma": [_i64],
     "pgb_grog_tc_timeouts": [_vp, _i64],
+    "pgb_grog_tc_wait_limit": [_i64, _vp],
+    "pgb_lsmr_u_update": [_vp, _vp, _i64, _vp, _vp, _vp],
+    "pgb_lsmr_u_scale": [_vp, _i64, _vp, _vp],
+    "pgb_lsmr_v_full": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],
+    "pgb_lsmr_scalars": [_vp, _vp],
+    "pgb_lsmr_vec_update": [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp],
     "pgb_coil_covariance": [_vp, _i64, _i64, _vp, _vp],
     "pgb_coil_cross_covariance": [_vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_coil_compress": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
@@ -155,6 +161,7 @@ _SIZE_FUNCS = {
     "pgb_grog_v8_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_grog_tc_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_reduce_scratch_bytes": [],
+    "pgb_lsmr_scratch_bytes": [],
 }
 
 _lib = None
@@ -206,6 +213,28 @@ def call(name: str, *args) -> None:
     """Call ``name`` with ``args`` and raise RuntimeError on a non-zero status."""
     st = getattr(load_library(), name)(*args)
     check(st, name)
+
+
+def tc_timeouts(reset: bool = True) -> int:
+    """Tile waits of the tensor-core adjoint that gave up since the last reset
+    (device counter; the read is synchronous)."""
+    n = ctypes.c_int64(0)
+    call("pgb_grog_tc_timeouts", ctypes.byref(n), 1 if reset else 0)
+    return int(n.value)
+
+
+def check_tc_timeouts(what: str) -> None:
+    """Raise RuntimeError if a tensor-core tile wait gave up since the last
+    check.  A CTA whose wait gives up returns without writing the rest of its
+    results, so the output of the call that launched it is incomplete.  Reads
+    and resets the counter; the caller synchronises the launching stream
+    first."""
+    n = tc_timeouts(reset=True)
+    if n:
+        raise RuntimeError(
+            f"{what}: {n} tensor-core tile wait(s) timed out; the result is incomplete "
+            "(the brick tiles' tensor copies did not complete within the spin limit)"
+        )
 
 
 def stream_ptr(device=None) -> int:

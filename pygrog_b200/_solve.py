@@ -16,9 +16,10 @@ reference recurrence with torch tensors (inner products in FP64).
 
 from __future__ import annotations
 
-__all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG", "BatchedDeviceCG"]
+__all__ = ["cg", "lsmr", "solve", "SolveMixin", "DeviceCG", "BatchedDeviceCG", "DeviceLSMR"]
 
 import gc
+import math
 import weakref
 from collections.abc import Callable
 from typing import Any
@@ -320,6 +321,118 @@ def cg(
     return x.to(src_dev) if isinstance(x, torch.Tensor) else x
 
 
+class DeviceLSMR:
+    """LSMR state for one right-hand side on the device (``_solvers.py:145-262``).
+
+    Vectors are complex64 device tensors; every scalar of the recurrence is
+    FP64 in a device block (``include/pygrog_b200.h``, ``pgb_lsmr_*``), the
+    two branch tests and the stopping test are device flags, so an iteration
+    issues no host synchronisation and can be captured in a CUDA graph and
+    replayed (iterations after the stopping test leave the state unchanged).
+    The operator's ``forward`` / ``adjoint`` are called on device tensors.
+    """
+
+    def __init__(self, op, b: torch.Tensor, damp: float, tol: float, x0: torch.Tensor | None = None):
+        self.op = op
+        dev = b.device
+        st = _lib.stream_ptr(dev)
+        if x0 is not None:
+            b = b - op.forward(x0)
+        beta = float(torch.linalg.vector_norm(b.to(torch.complex128)))  # set-up syncs only
+        self.trivial = None
+        if beta == 0.0:
+            self.trivial = x0.clone() if x0 is not None else op.adjoint(b)
+            return
+        self.u = (b / beta).to(torch.complex64).contiguous()
+        v_full = op.adjoint(self.u)
+        alpha = float(torch.linalg.vector_norm(v_full.to(torch.complex128)))
+        if alpha == 0.0:
+            self.trivial = x0.clone() if x0 is not None else torch.zeros_like(v_full)
+            return
+        self.v = (v_full / alpha).to(torch.complex64).contiguous()
+        self.vf = torch.empty_like(self.v)
+        self.h = self.v.clone()
+        self.hbar = torch.zeros_like(self.v)
+        self.x = torch.zeros_like(self.v) if x0 is None else x0.to(dev, torch.complex64).clone()
+        self.nu, self.nv = int(self.u.numel()), int(self.v.numel())
+        lib = _lib.load_library()
+        self.scratch = torch.zeros((int(lib.pgb_lsmr_scratch_bytes()) + 7) // 8, dtype=torch.float64, device=dev)
+        sc = np.zeros(32, dtype=np.float64)
+        sc[[0, 1, 2, 3, 4, 5, 6, 7, 9, 11, 12]] = [alpha, beta, alpha, 1.0, 1.0, 1.0, 0.0, alpha * beta, beta,
+                                                  float(tol), float(damp)]
+        self.scal = torch.from_numpy(sc).to(dev)
+        self.graph = None
+        del st
+
+    def step(self):
+        st = _lib.stream_ptr(self.u.device)
+        Av = self.op.forward(self.v)
+        _lib.call("pgb_lsmr_u_update", self.u.data_ptr(), Av.data_ptr(), self.nu, self.scal.data_ptr(),
+                  self.scratch.data_ptr(), st)
+        _lib.call("pgb_lsmr_u_scale", self.u.data_ptr(), self.nu, self.scal.data_ptr(), st)
+        Atu = self.op.adjoint(self.u)
+        _lib.call("pgb_lsmr_v_full", self.vf.data_ptr(), Atu.data_ptr(), self.v.data_ptr(), self.nv,
+                  self.scal.data_ptr(), self.scratch.data_ptr(), st)
+        _lib.call("pgb_lsmr_scalars", self.scal.data_ptr(), st)
+        _lib.call("pgb_lsmr_vec_update", self.x.data_ptr(), self.h.data_ptr(), self.hbar.data_ptr(),
+                  self.v.data_ptr(), self.vf.data_ptr(), self.nv, self.scal.data_ptr(), st)
+
+    def capture(self):
+        """Capture one iteration in a CUDA graph (the operator runs once first,
+        on a copy of the state, so its FFT plans exist before the capture)."""
+        dev = self.u.device
+        state = (self.u, self.v, self.vf, self.h, self.hbar, self.x, self.scal)
+        saved = [t.clone() for t in state]
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            self.step()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        for t, v in zip(state, saved):
+            t.copy_(v)
+        g = torch.cuda.CUDAGraph()
+        gc_on = gc.isenabled()
+        gc.disable()  # no collection (and no CUDA frees it may trigger) while capturing
+        try:
+            with torch.cuda.graph(g):
+                self.step()
+        finally:
+            if gc_on:
+                gc.enable()
+        self.graph = g
+
+    def run(self, max_iter: int, callback: Callable | None = None, use_graph: bool = True) -> torch.Tensor:
+        if self.trivial is not None:
+            return self.trivial
+        if callback is None and use_graph and max_iter > 1:
+            if self.graph is None:
+                self.capture()
+            for _ in range(int(max_iter)):
+                self.graph.replay()
+            return self.x
+        for k in range(int(max_iter)):
+            self.step()
+            if callback is not None:
+                sc = self.scal.cpu()
+                if sc[18] != 0.0:
+                    callback(k, self.x, float(sc[19]))
+                if sc[10] != 0.0:
+                    break
+        return self.x
+
+
+def _device_lsmr_applicable(op, b) -> bool:
+    from .operator._masked_fft import MaskedFFT
+    from .operator._sparse_fft import SparseFFT
+
+    return (
+        isinstance(op, (SparseFFT, MaskedFFT))
+        and isinstance(b, torch.Tensor)
+        and b.device.type == "cuda"
+        and b.dtype == torch.complex64
+    )
+
+
 def lsmr(
     op: Any,
     b: torch.Tensor,
@@ -330,65 +443,70 @@ def lsmr(
     atol: float = 1e-6,
     btol: float = 1e-6,
     callback: Callable | None = None,
+    use_graph: bool = True,
 ) -> torch.Tensor:
     """LSMR (Fong & Saunders) for ``argmin ||A x - b||^2 + damp^2 ||x||^2``.
 
-    The recurrence of the reference (``_solvers.py:145-262``) with FP64
-    norms; vectors stay on the device.
+    The recurrence of the reference (``_solvers.py:145-262``).  On this
+    package's operators with complex64 device data it runs as
+    :class:`DeviceLSMR` (FP64 device scalars, no host synchronisation inside
+    the loop, one iteration replayed from a CUDA graph when there is no
+    callback); other operators use the same recurrence on the host with FP64
+    scalars.
     """
     b = _normalize_kspace_shape(op, b)
     src_dev = b.device
     if hasattr(op, "_cdev") and src_dev.type != "cuda":
         b = b.to(op._cdev)
+    if _device_lsmr_applicable(op, b):
+        x0d = None if x0 is None else torch.as_tensor(x0).to(b.device, torch.complex64)
+        solver = DeviceLSMR(op, b, damp, atol + btol, x0d)
+        return solver.run(int(max_iter), callback, use_graph).to(src_dev)
     if x0 is not None:
         b = b - op.forward(torch.as_tensor(x0).to(b.device))
 
     def nrm(t):
-        return torch.linalg.vector_norm(t.to(torch.complex128)).to(torch.float32)
+        return float(torch.linalg.vector_norm(t.to(torch.complex128)))
 
     beta = nrm(b)
-    if beta.item() == 0:
+    if beta == 0:
         out = torch.as_tensor(x0).clone() if x0 is not None else op.adjoint(b)
         return out.to(src_dev)
     u = b / beta
     v_full = op.adjoint(u)
     alpha = nrm(v_full)
-    if alpha.item() == 0:
+    if alpha == 0:
         out = torch.as_tensor(x0).clone() if x0 is not None else torch.zeros_like(v_full)
         return out.to(src_dev)
     v = v_full / alpha
     zetabar = alpha * beta
     alphabar = alpha
-    one = torch.tensor(1.0, dtype=alpha.dtype, device=alpha.device)
-    rho = one.clone()
-    rhobar = one.clone()
-    cbar = one.clone()
-    sbar = torch.zeros_like(one)
+    rho = rhobar = cbar = 1.0
+    sbar = 0.0
     h = v.clone()
     hbar = torch.zeros_like(v)
     x = torch.zeros_like(v) if x0 is None else torch.as_tensor(x0).to(v.device).clone()
-    normb = beta.clone()
-    zeta = zetabar
+    normb = beta
     for k in range(max_iter):
         u = op.forward(v) - alpha * u
         beta = nrm(u)
-        if beta.item() > 0:
+        if beta > 0:
             u = u / beta
             v_full = op.adjoint(u) - beta * v
             alpha = nrm(v_full)
-            if alpha.item() > 0:
+            if alpha > 0:
                 v = v_full / alpha
-        alphahat = torch.sqrt(alphabar * alphabar + damp * damp)
-        rhoold = rho.clone()
-        rho = torch.sqrt(alphahat * alphahat + beta * beta)
+        alphahat = math.sqrt(alphabar * alphabar + damp * damp)
+        rhoold = rho
+        rho = math.sqrt(alphahat * alphahat + beta * beta)
         c = alphahat / rho
         s = beta / rho
         thetanew = s * alpha
         alphabar = c * alpha
-        rhobarold = rhobar.clone()
+        rhobarold = rhobar
         thetabar = sbar * rho
         rhotemp = cbar * rho
-        rhobar = torch.sqrt(rhotemp * rhotemp + thetanew * thetanew)
+        rhobar = math.sqrt(rhotemp * rhotemp + thetanew * thetanew)
         cbar = rhotemp / rhobar
         sbar = thetanew / rhobar
         zeta = cbar * zetabar
@@ -396,7 +514,7 @@ def lsmr(
         hbar = h - (thetabar * rho / (rhoold * rhobarold)) * hbar
         x = x + (zeta / (rho * rhobar)) * hbar
         h = v - (thetanew / rho) * h
-        rel = (torch.abs(zetabar) / (normb + 1e-30)).item()
+        rel = abs(zetabar) / (normb + 1e-30)
         if callback is not None:
             callback(k, x, rel)
         if rel < atol + btol:

@@ -25,6 +25,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from .. import _lib
+
 __all__ = ["autotune_gridder", "clear_cache"]
 
 _CACHE: dict = {}
@@ -59,6 +61,8 @@ def _time(bp, data: torch.Tensor, G: int, reps: int, warmup: int):
         bp.adjoint(kg, out)
         ev[1].record()
         torch.cuda.synchronize(data.device)
+        if bp.tc is not None:  # a timed-out tile wait leaves the output incomplete: never time or pick it
+            _lib.check_tc_timeouts(f"autotune_gridder ({bp.mode})")
         if it >= warmup:
             ts.append(ev[0].elapsed_time(ev[1]))
     return float(np.median(ts)), kg, out

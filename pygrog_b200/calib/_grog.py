@@ -27,6 +27,7 @@ from __future__ import annotations
 __all__ = ["GrogInterpolator", "GrogPlan", "BrickPlan", "GrogGridder"]
 
 import math
+import os
 from types import SimpleNamespace
 
 import numpy as np
@@ -37,6 +38,8 @@ from ._grappa import KernelTable
 from ._plan6 import BrickPlan6, _sm_count, lane_chunk
 
 _DEFAULT_DEVICE = "cuda"
+# check the tensor-core timeout counter after every degrid (synchronising)
+_SYNC_CHECK = os.environ.get("PYGROG_B200_SYNC_CHECK", "0") not in ("", "0")
 
 
 # ---------------------------------------------------------------------------
@@ -1161,11 +1164,34 @@ class GrogInterpolator:
         for s in range(S):
             gs = g[:, s].contiguous()
             o = torch.empty(B, C, N, dtype=t.dtype, device=t.device) if S > 1 else out.view(B, C, N)
-            self._brick(s).adjoint(gs, o)
+            bp = self._brick(s)
+            bp.adjoint(gs, o)
+            if bp.tc is not None:
+                self._tc_pending = True
             if S > 1:
                 out[:, s] = o
         res = out.reshape(*batch, *s_shape, C, *spatial)
-        return self._to_host(res, is_numpy, src_dev)
+        host = self._to_host(res, is_numpy, src_dev)
+        if is_numpy or src_dev.type == "cpu" or _SYNC_CHECK:
+            self.check_errors()  # the launching stream has been synchronised (or is, here)
+        return host
+
+    def check_errors(self) -> None:
+        """Raise RuntimeError if a tensor-core adjoint launched by this
+        interpolator since the last check gave up waiting for a brick tile
+        (its result is then incomplete).  Synchronises the device.
+
+        ``degrid`` runs this check itself when it returns a host result, and
+        after every call when ``PYGROG_B200_SYNC_CHECK=1``; a device-resident
+        result is checked here, or by the next host-returning ``degrid``.
+        """
+        if not getattr(self, "_tc_pending", False):
+            return
+        if torch.cuda.is_current_stream_capturing():
+            return
+        torch.cuda.synchronize(self.device)
+        self._tc_pending = False
+        _lib.check_tc_timeouts("GrogInterpolator.degrid")
 
     # -- shot-by-shot ---------------------------------------------------------------
     def _grid_shot(self, data: torch.Tensor, shot_index: tuple) -> torch.Tensor:

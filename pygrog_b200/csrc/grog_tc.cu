@@ -131,6 +131,10 @@ __device__ __forceinline__ void wait_groups() {
 // stores / reduce-adds are bulk groups.  No multicast.
 __device__ int g_tc_timeouts;  // mbarrier waits that gave up (see pgb_grog_tc_timeouts)
 constexpr long long kSpinLimit = 1ll << 26;
+// Spin limit of the tile waits that gate compute (pgb_grog_tc_wait_limit sets
+// it; the default is kSpinLimit).  The drain of copies still in flight after a
+// wait gave up always uses kSpinLimit.
+__device__ long long g_tc_wait_limit = kSpinLimit;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -154,10 +158,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 // Bounded wait for the phase `parity` of `bar`; false (and a recorded
 // timeout) if it did not complete within the spin limit.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (long long i = 0; i < kSpinLimit; ++i)
+  const long long limit = g_tc_wait_limit;
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   if (threadIdx.x == 0) atomicAdd(&g_tc_timeouts, 1);
   return false;
+}
+// Bounded wait used only on the way out after a timeout: lets a tensor copy
+// that is still writing this CTA's shared memory finish before the CTA exits.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, unsigned parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return;
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void tma_load_tile(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
@@ -783,6 +794,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
   const Smem lay(CP, NS, nsteps, cells, cap, false, TMA);
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<float2*>(smem4) + lay.bar);
   unsigned phase = 0;  // bit k: parity of the next completion of bars[k]
+  unsigned pend = 0;   // bit k: a tensor copy into tile buffer k has been issued and not yet waited for
   __shared__ int s_ok;
   const int XS = cap + 4;
   float2* base = reinterpret_cast<float2*>(smem4);
@@ -807,6 +819,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
         mbar_expect_tx(bars + k, static_cast<unsigned>(C * cells * 8));
         tma_load_tile(tl, &tmap, 2 * x0, y0, z0, b * C, bars + k);
       }
+      pend |= 1u << k;  // block-uniform bookkeeping
       return;
     }
     for (int cl = tid; cl < cells; cl += kT) {
@@ -872,11 +885,21 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_degrid_tc_kernel(
     }
     const int u1 = ld_u(st.d1, more);
     const bool wait_tile = TMA && (st.i0.y & kFirst);  // this item's tile: its tensor copy
-    if (wait_tile && tid == 0) s_ok = mbar_wait(bars + par, (phase >> par) & 1) ? 1 : 0;
+    if (wait_tile && tid == 0) {
+      s_ok = mbar_wait(bars + par, (phase >> par) & 1) ? 1 : 0;
+      if (!s_ok) {  // give up on this CTA, but let every copy still in flight land first
+        for (int k = 0; k < 2; ++k)
+          if (pend & (1u << k)) mbar_drain(bars + k, (phase >> k) & 1);
+      }
+    }
     __syncthreads();  // tile of this brick complete; previous results flushed
     if (wait_tile) {
-      if (!s_ok) return;  // block-uniform: the copy never completed (recorded in g_tc_timeouts)
+      if (!s_ok) {  // block-uniform: the copy did not complete in time (counted in g_tc_timeouts)
+        wait_groups<0>();  // this thread's metadata copies, too
+        return;
+      }
       phase ^= 1u << par;
+      pend &= ~(1u << par);
     }
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
@@ -1266,6 +1289,19 @@ int pgb_grog_tc_use_tma(int64_t enable) {
   const int prev = g_use_tma ? 1 : 0;
   if (enable >= 0) g_use_tma = enable != 0;
   return prev;
+}
+
+int pgb_grog_tc_wait_limit(int64_t limit, int64_t* previous) {
+  clear_error();
+  PGB_REQUIRE(limit >= -1, PGB_ERR_INVALID, "grog_tc_wait_limit: limit must be >= 0, or -1 for the default");
+  long long prev = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&prev, g_tc_wait_limit, sizeof(prev));
+  PGB_REQUIRE(e == cudaSuccess, PGB_ERR_CUDA, "grog_tc_wait_limit: %s", cudaGetErrorString(e));
+  if (previous) *previous = prev;
+  const long long v = limit < 0 ? kSpinLimit : static_cast<long long>(limit);
+  e = cudaMemcpyToSymbol(g_tc_wait_limit, &v, sizeof(v));
+  PGB_REQUIRE(e == cudaSuccess, PGB_ERR_CUDA, "grog_tc_wait_limit: %s", cudaGetErrorString(e));
+  return PGB_OK;
 }
 
 int pgb_grog_tc_timeouts(int64_t* count, int64_t reset) {

@@ -10,6 +10,8 @@
 // Scalar block (double[kScalars]), device memory owned by the caller:
 //   [0] rz_old   [1] pAp   [2] rr (|r|^2)   [3] r0_norm   [4] rel   [5] done
 //   [6] tol      [7] spare
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -348,9 +350,33 @@ namespace {
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+void* g_noalloc_ctx[kNoAllocMaxDevices] = {};  // context the cached address belongs to
 
-// Device address of g_dot_rows_scratch on the current device, looked up once
-// per device (with that device current) and cached.
+// The calling thread's current driver context (nullptr when none is current
+// yet, or when the driver entry point is unavailable).
+void* current_context() {
+  using CtxGetCurrent = CUresult (*)(CUcontext*);
+  static CtxGetCurrent get = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get = reinterpret_cast<CtxGetCurrent>(fn);
+    else
+      cudaGetLastError();
+  }
+  CUcontext c = nullptr;
+  if (get == nullptr || get(&c) != CUDA_SUCCESS) return nullptr;
+  return static_cast<void*>(c);
+}
+
+// Device address of g_dot_rows_scratch on the current device, looked up with
+// that device current and cached per (device, context): after
+// cudaDeviceReset the primary context, and with it the address, is new, so
+// a changed context triggers a fresh lookup.
 int noalloc_scratch(double** ptr) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -361,7 +387,8 @@ int noalloc_scratch(double** ptr) {
   PGB_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, PGB_ERR_RANGE,
               "dot_f64_noalloc: device ordinal %d above the supported %d", dev, kNoAllocMaxDevices);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  void* ctx = current_context();
+  if (!g_noalloc_ptr[dev] || ctx == nullptr || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_dot_rows_scratch);
     if (e != cudaSuccess || p == nullptr) {
@@ -370,6 +397,7 @@ int noalloc_scratch(double** ptr) {
       return PGB_ERR_CUDA;
     }
     g_noalloc_ptr[dev] = static_cast<double*>(p);
+    g_noalloc_ctx[dev] = current_context();  // the lookup made the primary context current
   }
   *ptr = g_noalloc_ptr[dev];
   return PGB_OK;

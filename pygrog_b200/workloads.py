@@ -159,13 +159,41 @@ def ndft2d(coil_img: np.ndarray, coords: np.ndarray, snr_db: float = 30.0, seed:
     return out.reshape(C, *coords.shape[:-1]).astype(np.complex64)
 
 
+def ndft2d_device(coil_img: np.ndarray, coords: np.ndarray, device, noise: float = 0.01,
+                  seed: int = 1002) -> np.ndarray:
+    """Direct NDFT of coil images at ``coords`` in FP64 on ``device`` (torch
+    complex128, separable GEMMs), plus complex Gaussian noise of standard
+    deviation ``noise`` x the RMS of the signal; complex64 ``(C, *coords.shape[:-1])``."""
+    import torch
+
+    C, n, _ = coil_img.shape
+    k = torch.as_tensor(coords.reshape(-1, 2), dtype=torch.float64, device=device)
+    pos = torch.arange(n, dtype=torch.float64, device=device) - n // 2
+    ex = torch.exp(-2j * math.pi * torch.outer(k[:, 0], pos) / n)  # (M, n) along axis 0
+    ey = torch.exp(-2j * math.pi * torch.outer(k[:, 1], pos) / n)
+    img = torch.as_tensor(coil_img, dtype=torch.complex128, device=device)
+    out = torch.empty(C, k.shape[0], dtype=torch.complex128, device=device)
+    for c in range(C):
+        out[c] = ((ex @ img[c]) * ey).sum(1) / n
+    rms = float(out.abs().square().mean().sqrt())
+    rng = np.random.default_rng(seed + 1)
+    sig = noise * rms / math.sqrt(2.0)
+    nz = sig * (rng.standard_normal(out.shape) + 1j * rng.standard_normal(out.shape))
+    res = out.cpu().numpy() + nz
+    return res.reshape(C, *coords.shape[:-1]).astype(np.complex64)
+
+
 def config1_geometry(n_spokes: int = 20000, n_readout: int = 384, n: int = 192):
     """Kooshball trajectory of the 3-D roofline configuration."""
     return kooshball(n_spokes, n_readout, n / 2.0)
 
 
-def config2(seed: int = 1002) -> Workload:
-    """CG-SENSE: 320^2, spiral 24 x 4096, 16 coils, oversamp 2, kernel_width 2."""
+def config2(seed: int = 1002, ndft_device=None) -> Workload:
+    """CG-SENSE: 320^2, spiral 24 x 4096, 16 coils, oversamp 2, kernel_width 2.
+
+    With ``ndft_device`` the k-space is the FP64 NDFT of the phantom's coil
+    images computed on that device, plus 1% complex Gaussian noise; otherwise
+    seeded complex Gaussian samples of the same shape."""
     rng = np.random.default_rng(seed)
     n, C = 320, 16
     coords = spiral2d(24, 4096, n / 2.0)
@@ -173,7 +201,10 @@ def config2(seed: int = 1002) -> Workload:
     maps = gaussian_coils((n, n), C, rng)
     coil_img = maps * img
     acr = center_crop(centered_fft(coil_img, axes=(-2, -1)), 24, 2).astype(np.complex64)
-    data = (rng.standard_normal((C, 24, 4096)) + 1j * rng.standard_normal((C, 24, 4096))).astype(np.complex64)
+    if ndft_device is not None:
+        data = ndft2d_device(coil_img, coords, ndft_device, 0.01, seed)
+    else:
+        data = (rng.standard_normal((C, 24, 4096)) + 1j * rng.standard_normal((C, 24, 4096))).astype(np.complex64)
     return Workload("c2", (n, n), coords, 2.0, 2, "circle", 1, 1e-3, acr, data, maps, (n, n))
 
 

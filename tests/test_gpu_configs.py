@@ -1,0 +1,132 @@
+"""Parity at the full sizes of the benchmark configurations.
+
+c0  256^2 golden-angle radial, 64 spokes x 512 samples, 8 coils, 5x5 square
+    kernel, oversampling 1, table precision 2, k-space = FP64 NDFT of a seeded
+    ellipse phantom times Gaussian coil maps plus noise at 30 dB.  Plan keys
+    (``target_idx``) and quantised shift indices bit-exact against the oracle
+    plan; ``interpolate``, ``interpolate(grid=True)`` and ``degrid`` within
+    1e-5 (relative L2) of the reference's own compiled CPU kernels
+    (``oracle/_ref``, driven in the reference's call order by
+    ``oracle/ref_cpu.py``: ``calib/_grog.py:437-555, 668-695, 736-902``).
+c1  192^3 kooshball, 20,000 spokes x 384 samples, 12 virtual coils (PCA of 32
+    Gaussian coils), sphere kernel width 2, precision 1: the tensor-core
+    (bf16x3, FP32 accumulate) forward and adjoint through the public API
+    within 1e-4 of an FP64 restatement of the same operator (complex128).
+c2  320^2 variable-density spiral, 24 x 4096 samples, 16 coils, oversampling 2
+    (Toeplitz PSF on 640^2), k-space = FP64 NDFT of the phantom plus 1%
+    noise: SparseFFT adjoint within 1e-5 and ``solve(method="cg",
+    max_iter=30, damp=1e-3)`` within 1e-4 of an FP64 CG-SENSE of the oracle
+    (``operator/_sparse_fft.py:574-621``, ``_toep/_grog_toep.py:154-209``,
+    ``_solve/_solvers.py:49-139``); ``solve(method="lsmr", max_iter=20,
+    damp=1e-3)`` on the non-Toeplitz operator within 1e-4 of an FP64 LSMR of
+    the oracle (``_solve/_solvers.py:145-262``).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import grog as og
+from oracle import operators as oo
+from pygrog_b200.calib import GrogInterpolator
+
+pytestmark = pytest.mark.gpu
+
+
+def test_config0_matches_reference_cpu_path(cuda):
+    from oracle.ref_cpu import ReferenceCPU
+    from pygrog_b200.workloads import config0
+
+    w = config0(ndft=True)
+    C = w.data.shape[0]
+    ref = ReferenceCPU(w.shape, w.coords, w.oversamp, w.kernel_width, w.kernel_shape, w.acr, w.precision, w.lamda)
+    assert ref.kind == "reference", "the reference's compiled CPU kernels (oracle/_ref) must be built"
+    g = GrogInterpolator(shape=w.shape, coords=w.coords, oversamp=w.oversamp, kernel_width=w.kernel_width,
+                         kernel_shape=w.kernel_shape, device=cuda)
+    assert tuple(g.plan.grid_shape) == (256, 256) and int(g.plan.target_idx.shape[-1]) == 25
+    np.testing.assert_array_equal(g.plan.target_idx.cpu().numpy(), ref.plan["target_idx"])
+    g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)
+    np.testing.assert_array_equal(g._interp_idx.cpu().numpy(), ref.interp_idx)
+    assert rel_l2(g._interp_kernel.numpy(), ref.table) < 1e-5
+
+    flat = w.data.reshape(C, -1)
+    sp = g.interpolate(w.data)
+    assert sp.shape == (C, flat.shape[1] * 25)
+    assert rel_l2(sp, ref.interpolate(flat)) < 1e-5
+
+    kg, mplan = g.interpolate(w.data, grid=True)
+    kg_ref = ref.forward(flat)
+    assert rel_l2(kg.reshape(C, -1), kg_ref) < 1e-5
+    dens = np.zeros(ref.G, dtype=np.float64)
+    np.add.at(dens, ref.fplan["indices"], ref.fplan["sqrt_weights"].astype(np.float64) ** 2)
+    np.testing.assert_allclose(np.asarray(mplan.density).reshape(-1), dens, rtol=1e-5, atol=1e-6)
+    np.testing.assert_array_equal(np.asarray(mplan.mask).reshape(-1), (dens > 0).astype(np.float32))
+    assert rel_l2(g.grid(w.data).reshape(C, -1), kg_ref) < 1e-5
+
+    back = g.degrid(kg)
+    assert rel_l2(back.reshape(C, -1), ref.adjoint(np.ascontiguousarray(kg.reshape(C, -1)))) < 1e-5
+
+
+def test_config1_tensor_core_path_matches_fp64(cuda):
+    import bench
+
+    g, coords, acr, data = bench.build_workload(cuda)
+    C, N = int(data.shape[1]), int(data.shape[2])
+    assert (C, N) == (12, 20000 * 384)
+    g.gridder_mode = "tc"
+    x = data[0].reshape(C, 20000, 384)
+    kg = g.grid(x)
+    assert g._brick(0).mode == "tc" and tuple(kg.shape) == (C, 192, 192, 192)
+    chk = bench.Fp64Check(g, N, C)
+    ref = chk.forward(data[0])
+    err_f = chk.rel(kg.reshape(C, -1), ref)
+    del ref
+    back = g.degrid(kg)
+    err_a = chk.rel(back.reshape(C, -1), chk.adjoint(kg.reshape(C, -1)))
+    assert err_f < 1e-4, f"forward {err_f:.3e}"
+    assert err_a < 1e-4, f"adjoint {err_a:.3e}"
+
+
+def test_config2_cg_sense_matches_fp64(cuda):
+    from pygrog_b200.operator import SparseFFT
+    from pygrog_b200.workloads import config2
+
+    w = config2(ndft_device=cuda)
+    C = w.data.shape[0]
+    g = GrogInterpolator(shape=w.shape, coords=w.coords, oversamp=w.oversamp, kernel_width=w.kernel_width,
+                         kernel_shape=w.kernel_shape, device=cuda)
+    g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)
+    smaps = torch.from_numpy(w.smaps.astype(np.complex64)).to(cuda)
+    op = SparseFFT(plan=g.plan, smaps=smaps, toeplitz=True)
+    assert tuple(op.grid_shape) == (640, 640)
+    data = torch.from_numpy(w.data).to(cuda)
+    sparse = torch.as_tensor(g.interpolate(data))
+    b = sparse * g.plan.pre_weights.unsqueeze(0)
+    AHb = op.adjoint(b)
+    x = op.solve(b.reshape(C, *op.natural_shape), method="cg", max_iter=30, damp=1e-3, tol=0.0)
+
+    plan = g.plan
+    N = int(np.prod(w.data.shape[1:]))
+    table = g._interp_kernel.numpy().astype(np.complex128)
+    idx = g._interp_idx.cpu().numpy().reshape(N, -1)
+    rep = og.interpolate(w.data.reshape(1, C, N).astype(np.complex128), idx, table)[0]
+    ip = plan.inv_perm.cpu().numpy()
+    idx_nat = plan.indices.cpu().numpy()[ip]
+    sw_nat = plan.sqrt_weights.cpu().numpy().astype(np.float64)[ip]
+    sm = w.smaps.astype(np.complex128)
+    grid, img = tuple(op.grid_shape), tuple(op.image_shape)
+    AHb_ref = oo.sparse_adjoint(rep * sw_nat, idx_nat, sw_nat, grid, img, sm)
+    assert rel_l2(AHb.cpu().numpy(), AHb_ref) < 1e-5
+    psf = oo.psf(idx_nat, sw_nat, grid)
+    x_ref = oo.cg(lambda v: oo.toeplitz_normal(v, psf, grid, img, sm), AHb_ref, damp=1e-3, max_iter=30)
+    err = rel_l2(x.cpu().numpy(), x_ref)
+    assert err < 1e-4, f"CG-SENSE {err:.3e}"
+
+    opn = SparseFFT(plan=g.plan, smaps=smaps, toeplitz=False)
+    xl = opn.solve(b.reshape(C, *opn.natural_shape), method="lsmr", max_iter=20, damp=1e-3)
+    b_ref = (rep * sw_nat).reshape(C, -1)
+    xl_ref = oo.lsmr(lambda v: oo.sparse_forward(v, idx_nat, sw_nat, grid, img, sm),
+                     lambda u: oo.sparse_adjoint(u, idx_nat, sw_nat, grid, img, sm), b_ref, damp=1e-3, max_iter=20)
+    err_l = rel_l2(xl.cpu().numpy(), xl_ref)
+    assert err_l < 1e-4, f"LSMR {err_l:.3e}"

@@ -278,6 +278,39 @@ def test_tensor_core_fallback_paths_match(cuda):
     assert cnt[0] == 0
 
 
+def test_tensor_core_wait_timeout_raises(cuda):
+    """A tile wait that gives up is an error, not a silent partial result.
+
+    The adjoint's spin limit is set to 0, so every tile wait gives up at once
+    (the tensor copies themselves complete normally and are drained before
+    the CTA leaves; nothing faults).  degrid must raise, the counter must be
+    reset by the raise, and with the default limit restored the same call
+    gives the full result again."""
+    import ctypes
+
+    from pygrog_b200 import _lib
+
+    n = 48
+    coords, calib, data = _random_case(2, n, 24, 96, 8, 1.0, 2, "circle", 1, seed=3)
+    g = GrogInterpolator(shape=(n, n), coords=coords, oversamp=1.0, kernel_width=2, device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    g.gridder_mode = "tc"
+    kg = g.grid(data)
+    good = g.degrid(kg)
+    assert _lib.tc_timeouts(reset=False) == 0
+    prev = ctypes.c_int64(0)
+    _lib.call("pgb_grog_tc_wait_limit", 0, ctypes.byref(prev))
+    try:
+        with pytest.raises(RuntimeError, match="timed out"):
+            g.degrid(kg)
+    finally:
+        _lib.call("pgb_grog_tc_wait_limit", -1, None)
+    assert prev.value > 0
+    assert _lib.tc_timeouts(reset=False) == 0  # the raise consumed the count
+    again = g.degrid(kg)
+    assert rel_l2(again, good) == 0.0
+
+
 def test_autotuner_picks_a_valid_gridder(cuda):
     """The autotuner times the families that fit, installs the fastest, and
     the installed gridder still matches the FP64 oracle within its family's

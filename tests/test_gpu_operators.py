@@ -81,6 +81,30 @@ def test_cg_and_lsmr_match_reference(cuda, name):
     assert op.toeplitz is True and opn.toeplitz is False
 
 
+def test_device_lsmr_graph_eager_and_early_stop(cuda):
+    """Device LSMR: the graph-replayed iteration and the eager loop agree; a
+    stopping tolerance freezes the state at the iteration where the
+    reference's loop breaks (same result as that many iterations run alone),
+    and the eager loop's callback sees the reference's relative residuals."""
+    from pygrog_b200._solve import lsmr
+
+    z, g, C = _plan("op2d", cuda)
+    sm = torch.from_numpy(z["in_smaps"])
+    opn = SparseFFT(plan=g.plan, smaps=sm, toeplitz=False)
+    bn = torch.from_numpy(z["in_b"]).reshape(C, *opn.natural_shape).to(cuda)
+    xg = lsmr(opn, bn, damp=1e-3, max_iter=12)
+    xe = lsmr(opn, bn, damp=1e-3, max_iter=12, use_graph=False)
+    assert rel_l2(xe.cpu().numpy(), xg.cpu().numpy()) < 1e-6
+    seen = []
+    lsmr(opn, bn, damp=1e-3, max_iter=40, callback=lambda k, x, r: seen.append(r))
+    assert len(seen) > 6
+    tol = seen[5] * 1.0000001  # the test fires at iteration 5 at the latest (0-based)
+    k_stop = next(k for k, r in enumerate(seen) if r < tol)
+    x_tol = lsmr(opn, bn, damp=1e-3, max_iter=40, atol=tol / 2, btol=tol / 2)
+    x_k = lsmr(opn, bn, damp=1e-3, max_iter=k_stop + 1)
+    assert rel_l2(x_tol.cpu().numpy(), x_k.cpu().numpy()) < 1e-6
+
+
 def test_cg_early_exit_matches_break(cuda):
     z, g, C = _plan("op2d", cuda)
     sm = torch.from_numpy(z["in_smaps"])

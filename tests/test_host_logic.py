@@ -410,3 +410,30 @@ def test_cell_row_plan_packs_runs_into_m_tiles():
     qm = q.meta.numpy()
     assert sorted(zip((meta[valid, 0] & 0xFFFF).tolist(), p.w.numpy()[valid].round(6).tolist())) == \
         sorted(zip((qm[:, 0] & 0xFFFF).tolist(), q.w.numpy().round(6).tolist()))
+
+
+def test_tensor_core_timeout_count_raises(monkeypatch):
+    """A non-zero tile-wait timeout count becomes a RuntimeError at the check
+    points (counter read mocked: no device here); a zero count passes and a
+    pending check is consumed once."""
+    from pygrog_b200 import _lib
+
+    counts = [2]
+    monkeypatch.setattr(_lib, "tc_timeouts", lambda reset=True: counts.pop(0) if counts else 0)
+    with pytest.raises(RuntimeError, match="2 tensor-core tile wait"):
+        _lib.check_tc_timeouts("degrid")
+    _lib.check_tc_timeouts("degrid")  # counter now 0: no error
+
+    g = _grog.GrogInterpolator.__new__(_grog.GrogInterpolator)
+    g.device = torch.device("cpu")
+    monkeypatch.setattr(torch.cuda, "is_current_stream_capturing", lambda: False)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda device=None: None)
+    g.check_errors()  # nothing launched: no read at all
+    counts[:] = [1]
+    g._tc_pending = True
+    with pytest.raises(RuntimeError, match="GrogInterpolator.degrid: 1 tensor-core tile wait"):
+        g.check_errors()
+    assert g._tc_pending is False
+    counts[:] = [5]
+    g.check_errors()  # no launch since the last check: the counter is not read
+    assert counts == [5]

@@ -129,6 +129,18 @@ def test_oracle_cg_matches_reference(name):
     assert rel_l2(x, z["ref_cg"]) < 1e-4
 
 
+@pytest.mark.parametrize("name", ["op2d", "op3d"])
+def test_oracle_lsmr_matches_reference(name):
+    z, shape, img, p, idx, sw, C = _op_setup(name)
+    gs = tuple(p["grid_shape"])
+    sm = z["in_smaps"].astype(np.complex128)
+    x = oo.lsmr(lambda v: oo.sparse_forward(v, idx, sw, gs, img, sm),
+                lambda u: oo.sparse_adjoint(u, idx, sw, gs, img, sm),
+                z["in_b"].astype(np.complex128), damp=1e-3, max_iter=8)
+    # the reference iterates in complex64 with FP32 norms
+    assert rel_l2(x, z["ref_lsmr"]) < 1e-4
+
+
 def _sub_setup():
     z = golden("sub_sub2d.npz")
     _, shape, img, osf, C, K, T = parse_meta(z["meta"])

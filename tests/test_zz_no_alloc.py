@@ -60,3 +60,26 @@ def test_noalloc_matches_dot_f64_twice_in_a_row(cuda):
     a = torch.empty(3, 0, dtype=torch.complex64, device=cuda)
     out.fill_(1.0)
     assert torch.all(_dot_noalloc(a, a, out[:3], cuda) == 0)
+
+
+@pytest.mark.gpu
+def test_noalloc_back_to_back_on_one_stream(cuda):
+    """Several calls with different inputs queued on one stream with no host
+    synchronisation between them, then one sync: each call's kernel must see
+    the counters that its own clear left, so every output must still match
+    pgb_dot_f64."""
+    g = torch.Generator(device="cpu").manual_seed(11)
+    cases = [(7, 50_001), (MAX_ROWS, 2_053), (3, 300_007), (MAX_ROWS, 17), (1, 1)]
+    data = []
+    for rows, n in cases:
+        a = torch.randn(rows, n, dtype=torch.complex64, generator=g).to(cuda)
+        b = torch.randn(rows, n, dtype=torch.complex64, generator=g).to(cuda)
+        data.append((a, b, _dot_existing(a, b, cuda)))
+    torch.cuda.synchronize(cuda)
+    outs = [torch.full((a.shape[0],), float("nan"), dtype=torch.float64, device=cuda) for a, _, _ in data]
+    stream = _lib.stream_ptr(cuda)
+    for (a, b, _), out in zip(data, outs):
+        _lib.call("pgb_dot_f64_noalloc", a.data_ptr(), b.data_ptr(), a.shape[1], a.shape[0], out.data_ptr(), stream)
+    torch.cuda.synchronize(cuda)
+    for (_, _, ref), out in zip(data, outs):
+        torch.testing.assert_close(out.cpu(), ref, rtol=1e-12, atol=1e-9)
