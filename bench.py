@@ -646,7 +646,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--table-mode", default="tc",
-                    choices=["auto", "tc", "tc1", "v9", "v8", "v8pair", "v6", "v5", "v3", "smem", "factored", "global"],
+                    choices=["auto", "tc", "tc1", "v8", "v8pair", "v6", "global"],
                     help="gridder: tc = tensor-core bf16x3 (default), tc1 = bf16, v8 = FP32 CUDA cores, auto")
     ap.add_argument("--no-precision-modes", action="store_true", help="skip the FP32 / bf16 comparison")
     ap.add_argument("--autotune", action="store_true",
@@ -853,7 +853,7 @@ def main():
                              else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode + ("/pairs" if getattr(bp, "pairs", False) else ""), "kernels": list(bp.kernel_names()), "l2": f"inputs larger than L2 ({N * C * 8 / 1e6:.0f} MB samples, {G * C * 8 / 1e6:.0f} MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "kernels": list(bp.kernel_names()), "l2": f"inputs larger than L2 ({N * C * 8 / 1e6:.0f} MB samples, {G * C * 8 / 1e6:.0f} MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
             "fwd_ms": fwd_ms,

@@ -193,64 +193,6 @@ PGB_API int pgb_grog_degrid(const void* grid, int64_t G, void* out, int64_t N,
                     const pgb_brick_plan* plan, int accumulate,
                     const int32_t* zero_src, int64_t n_zero, void* stream);
 
-/* Factored-table variants of pgb_grog_grid / pgb_grog_degrid for tables that
- * split as T[e] = outer[e % n_outer] @ inner[e / n_outer] (3-D:
- * outer = Gx, inner[i*n + j] = Gy[j] @ Gz[i]; 2-D: outer = Gx, inner = Gy;
- * n_outer = 1 with outer = NULL means T = inner).  `inner` (n_inner, C, C)
- * is staged in shared memory by persistent CTAs; outer rows are applied once
- * per run of replicas sharing (e % n_outer, cell), so replicas inside each
- * brick must be sorted by (e % n_outer, cell).  The adjoint takes the
- * conjugate transposes inner_h / outer_h and applies outer_h first.
- * Requires pgb_grog_factored_smem_bytes(C, cells, n_inner) <= 227 KiB. */
-PGB_API size_t pgb_grog_factored_smem_bytes(int64_t C, int64_t cells, int64_t n_inner);
-PGB_API int pgb_grog_grid_factored(const void* data, int64_t N, void* grid, int64_t G,
-                                   const void* inner, int64_t n_inner, const void* outer,
-                                   int64_t n_outer, int64_t C, int64_t B,
-                                   const pgb_brick_plan* plan, void* stream);
-PGB_API int pgb_grog_degrid_factored(const void* grid, int64_t G, void* out, int64_t N,
-                                     const void* inner_h, int64_t n_inner,
-                                     const void* outer_h, int64_t n_outer, int64_t C,
-                                     int64_t B, const pgb_brick_plan* plan, int accumulate,
-                                     const int32_t* zero_src, int64_t n_zero, void* stream);
-
-/* Latency-hiding variants (C <= 16, bricks <= 512 cells, power-of-two brick
- * extents) used by the GROG operator whenever the table, or its inner
- * factor, fits in shared memory.  Persistent CTAs stage sub-chunks of 128
- * replicas (metadata and source samples) one step ahead in shared memory.
- * Per-replica metadata is pre-split at plan time:
- *   rep_meta = cell | inner << 11 | outer << 25.
- * The adjoint runs `primary` (the first valid replica of every sample,
- * stored) then `secondary` (any further replicas, accumulated atomically;
- * may be NULL); samples listed in zero_src have no valid replica and are
- * zeroed. */
-PGB_API size_t pgb_grog_v3_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int forward);
-PGB_API int pgb_grog_grid_v3(const void* data, int64_t N, void* grid, int64_t G,
-                             const void* inner, int64_t n_inner, const void* outer,
-                             int64_t n_outer, int64_t C, int64_t B,
-                             const pgb_brick_plan* plan, void* stream);
-PGB_API int pgb_grog_degrid_v3(const void* grid, int64_t G, void* out, int64_t N,
-                               const void* inner_h, int64_t n_inner, const void* outer_h,
-                               int64_t n_outer, int64_t C, int64_t B,
-                               const pgb_brick_plan* primary, const pgb_brick_plan* secondary,
-                               const int32_t* zero_src, int64_t n_zero, void* stream);
-
-/* One-lane-per-replica variants (C <= 16, power-of-two bricks of at most
- * 2048 cells): every lane applies the whole operator(s) of its replica from
- * shared memory; replicas inside each brick must be sorted by inner table
- * index (then outer index, then cell) so that a warp reads few distinct
- * operators.  Same metadata packing and adjoint passes as the v3 variants.
- * Shared memory: pgb_grog_v5_smem_bytes(C, cells, n_inner, n_outer). */
-PGB_API size_t pgb_grog_v5_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer);
-PGB_API int pgb_grog_grid_v5(const void* data, int64_t N, void* grid, int64_t G,
-                             const void* inner, int64_t n_inner, const void* outer,
-                             int64_t n_outer, int64_t C, int64_t B,
-                             const pgb_brick_plan* plan, void* stream);
-PGB_API int pgb_grog_degrid_v5(const void* grid, int64_t G, void* out, int64_t N,
-                               const void* inner_h, int64_t n_inner, const void* outer_h,
-                               int64_t n_outer, int64_t C, int64_t B,
-                               const pgb_brick_plan* primary, const pgb_brick_plan* secondary,
-                               const int32_t* zero_src, int64_t n_zero, void* stream);
-
 /* Operator-stationary variants (C <= 16, power-of-two bricks of at most
  * 4096 cells).  Replaces the per-replica operator application of
  * calib/_grog.py:1283-1295 fused with the scatter of
@@ -324,17 +266,6 @@ PGB_API int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N
                                int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C, int64_t B,
                                const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
                                const int32_t* zero_src, int64_t n_zero, void* stream);
-/* Two threads per replica (512-thread CTA, each thread C / 2 rows of every
- * product, halves joined with warp shuffles): even C only; otherwise the
- * same plans, contract and shared memory as the v8 entry points. */
-PGB_API int pgb_grog_grid_v9(const void* data, int64_t N, void* grid, int64_t G, const void* inner,
-                             int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
-                             const pgb_v6_plan* plan, void* stream);
-PGB_API int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h,
-                               int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C, int64_t B,
-                               const pgb_v6_plan* primary, const pgb_v6_plan* secondary,
-                               const int32_t* zero_src, int64_t n_zero, void* stream);
-
 /* Tensor-core (mma.sync bf16, fp32 accumulate) gridding: the same operator as
  * the table path of calib/_grog.py:1283-1295 + operator/_sparse_fft.py:416
  * (forward) and its adjoint, with the table applied in its exact eigen-factored

@@ -93,27 +93,6 @@ _SIGS = {
         _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _i32, _vp, _i64, _vp,
     ],
     "pgb_grog_expand": [_vp, _i64, _i32, _vp, _vp, _i64, _i64, _i64, _vp, _vp],
-    "pgb_grog_grid_factored": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
-    ],
-    "pgb_grog_degrid_factored": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _i32,
-        _vp, _i64, _vp,
-    ],
-    "pgb_grog_grid_v3": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
-    ],
-    "pgb_grog_degrid_v3": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC),
-        ctypes.POINTER(BrickPlanC), _vp, _i64, _vp,
-    ],
-    "pgb_grog_grid_v5": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC), _vp,
-    ],
-    "pgb_grog_degrid_v5": [
-        _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, ctypes.POINTER(BrickPlanC),
-        ctypes.POINTER(BrickPlanC), _vp, _i64, _vp,
-    ],
     "pgb_fft_expand": [_vp, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _f32, _i32, _vp],
     "pgb_fft_combine": [_vp, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _f32, _vp, _f32, _vp],
     "pgb_sparse_scatter": [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _vp],
@@ -126,8 +105,6 @@ _SIGS = {
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
     "pgb_grog_grid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
     "pgb_grog_degrid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
-    "pgb_grog_grid_v9": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
-    "pgb_grog_degrid_v9": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _vp],
     "pgb_subspace_scatter": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_subspace_gather": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _vp],
     "pgb_psf_apply_kk": [_vp, _vp, _i64, _i64, _i64, _i64, _vp],
@@ -154,9 +131,6 @@ _SIGS = {
     "pgb_coil_compress_tc": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],
 }
 _SIZE_FUNCS = {
-    "pgb_grog_factored_smem_bytes": [_i64, _i64, _i64],
-    "pgb_grog_v3_smem_bytes": [_i64, _i64, _i64, _i32],
-    "pgb_grog_v5_smem_bytes": [_i64, _i64, _i64, _i64],
     "pgb_grog_v6_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_grog_v8_smem_bytes": [_i64, _i64, _i64, _i64, _i64],
     "pgb_grog_tc_smem_bytes": [_i64, _i64, _i64, _i64, _i64],

@@ -473,19 +473,15 @@ class GrogGridder:
       ``"v8"``        C <= 16: one lane per replica on balanced sub-chunk
                       streams, replicas ordered (outer, inner, cell) so
                       operator loads are conflict-free or broadcast; the
-                      forward sums each cell's replicas without atomics;
+                      forward sums each cell's replicas without atomics
+                      (the FP32 default);
       ``"v8pair"``    the v8 adjoint with the v6 forward;
-      ``"v9"``        v8 with two threads per replica (512-thread CTAs, each
-                      thread half the rows of every product), even C;
       ``"v6"``        C <= 16: operator-stationary slots (outer factor rows
                       in registers along sorted runs, inner factor or whole
                       table in shared memory), dynamic work queue;
-      ``"v5"``        C <= 16: one lane per replica;
-      ``"v3"``        C <= 16: whole table or its inner factor in shared
-                      memory, sub-chunks staged ahead in shared memory by
-                      persistent CTAs, adjoint as store pass + atomic pass;
-      ``"smem"`` / ``"factored"``  same tables, one slot pipeline per CTA;
-      ``"global"``    table read through L1/L2 (any C <= 32, K < 2^20).
+      ``"global"``    table read through L1/L2 (any C <= 32, K < 2^20): the
+                      FP32 gridder above 16 coils or when no table fits
+                      shared memory.
     With a factored table ``T[e] = outer[e % n] @ inner[e // n]``, the outer
     factor is applied once per run of replicas sharing (outer index, cell).
     """
@@ -494,9 +490,6 @@ class GrogGridder:
     # v8 plans: deal replicas round-robin over inner residues q mod 8 inside
     # outer runs (BrickPlan6 lane_order): fewer shared-memory bank conflicts
     LANE_ORDER_V8 = True
-    # two threads per replica (v9 entry points) by default for even C: measured
-    # slower than one (1.90 / 1.24 against 1.86 / 1.22 ms on the 192^3 kooshball)
-    PAIRS_DEFAULT = False
     # v8 forward: longest run of one cell's replicas summed by one thread
     SEG_LEN_V8 = 24
     BRICKS2 = ((1, 16, 32), (1, 16, 16), (1, 8, 16), (1, 8, 8))
@@ -519,15 +512,6 @@ class GrogGridder:
             return
         n_fact = int(factors[1].shape[0]) if factors is not None else None
 
-        def v3_fits(n_inner, br):
-            cells = br[0] * br[1] * br[2]
-            return (lib.pgb_grog_v3_smem_bytes(C, cells, n_inner, 1) <= _SMEM_V3
-                    and lib.pgb_grog_v3_smem_bytes(C, cells, n_inner, 0) <= _SMEM_V3)
-
-        def v5_fits(n_inner, n_outer, br):
-            cells = br[0] * br[1] * br[2]
-            return lib.pgb_grog_v5_smem_bytes(C, cells, n_inner, n_outer) <= _SMEM_V3
-
         def v6_fits(n_in, n_out, br, sub):
             cells = br[0] * br[1] * br[2]
             return lib.pgb_grog_v6_smem_bytes(C, cells, n_in, n_out, sub) <= _SMEM_V3
@@ -539,11 +523,7 @@ class GrogGridder:
         chosen = None
         self.sub_cap = None
         self.fwd6 = None  # (brick, sub_cap, factored) of the v6 forward used with the v8 adjoint
-        # v8 family with two threads per replica (v9 entry points)
-        self.pairs = C % 2 == 0 and (mode == "v9" or (mode is None and self.PAIRS_DEFAULT))
-        if mode == "v9" and C % 2:
-            raise ValueError("v9 kernels need an even coil count")
-        if mode in (None, "v8", "v8pair", "v9") and C <= 16:
+        if mode in (None, "v8", "v8pair") and C <= 16:
             n_out_f = int(factors[0].shape[0]) if factors is not None else None
             for sub in (256, 192, 128):
                 for br in cand:
@@ -580,38 +560,15 @@ class GrogGridder:
                         break
                 if chosen is not None:
                     break
-        if chosen is None and mode in (None, "v5") and C <= 16:
-            for br in cand:
-                if v5_fits(K, 1, br) and K <= 16384:
-                    chosen = ("v5", br, False)
-                    break
-                if (n_fact is not None and n_fact <= 16384 and int(factors[0].shape[0]) <= 128
-                        and v5_fits(n_fact, int(factors[0].shape[0]), br)):
-                    chosen = ("v5", br, True)
-                    break
-        if chosen is None and mode in (None, "v3") and C <= 16:
-            for br in cand:
-                if v3_fits(K, br):
-                    chosen = ("v3", br, False)
-                    break
-                if n_fact is not None and n_fact <= 16384 and int(factors[0].shape[0]) <= 128 and v3_fits(n_fact, br):
-                    chosen = ("v3", br, True)
-                    break
         if chosen is None:
-            if mode in ("v3", "v5", "v6", "v8", "v8pair", "v9"):
+            if mode in ("v6", "v8", "v8pair"):
                 raise ValueError(f"{mode} kernels need C <= 16 and a table that fits shared memory")
-            br = cand[0] if ndim == 3 and C <= 16 or ndim == 2 and C <= 16 else (
-                (4, 8, 8) if ndim == 3 else (1, 16, 16))
+            if mode not in (None, "global"):
+                raise ValueError(f"unknown gridder mode {mode!r} (tc, tc1, v8, v8pair, v6, global)")
+            br = cand[0] if C <= 16 else ((4, 8, 8) if ndim == 3 else (1, 16, 16))
             if brick is not None:
                 br = tuple(brick)
-            cells = br[0] * br[1] * br[2]
-            fit = lambda n: lib.pgb_grog_factored_smem_bytes(C, cells, n) <= _SMEM_BUDGET  # noqa: E731
-            if mode in (None, "smem") and fit(K):
-                chosen = ("smem", br, False)
-            elif mode in (None, "factored") and n_fact is not None and fit(n_fact):
-                chosen = ("factored", br, True)
-            else:
-                chosen = ("global", br, False)
+            chosen = ("global", br, False)
         self.mode, brick, factored = chosen
         self.brick = brick
         dev = target_idx.device
@@ -629,8 +586,7 @@ class GrogGridder:
             self.outer = self.outer_h = None
         self.plan2 = None  # adjoint secondary replicas (v3 / v5 / v6 / v8)
         if self.mode == "v8":
-            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap, lane_order=self.LANE_ORDER_V8,
-                       pair_lanes=self.pairs)
+            kw8 = dict(brick=brick, n_outer=self.n_outer, sub_cap=self.sub_cap, lane_order=self.LANE_ORDER_V8)
             if self.fwd6 is not None:
                 br6, sub6, _ = self.fwd6
                 self.inner_lc = lane_chunk(self.inner)
@@ -657,16 +613,9 @@ class GrogGridder:
             if self.plan.n_valid > self.adj_plan.n_valid:
                 self.plan2 = BrickPlan6(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kw6)
             return
-        pack = "split" if self.mode in ("v3", "v5") else "wide"
-        kwargs = dict(brick=brick, chunk=chunk, n_outer=self.n_outer, pack=pack,
-                      order="inner" if self.mode == "v5" else "cell")
+        kwargs = dict(brick=brick, chunk=chunk, n_outer=self.n_outer, pack="wide", order="cell")
         self.plan = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, **kwargs)
         self.adj_plan = self.plan
-        if self.mode in ("v3", "v5"):
-            first = _first_valid_mask(target_idx, kw)
-            self.adj_plan = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=first, **kwargs)
-            if self.plan.n_valid > self.adj_plan.n_valid:
-                self.plan2 = BrickPlan(target_idx, interp_idx, rep_weight, kw, grid_shape, mask=~first, **kwargs)
 
     def _init_tc(self, mode, tc_ops, target_idx, interp_idx, rep_weight, kw, grid_shape, cand, lib):
         """Tensor-core gridder (``csrc/grog_tc.cu``): sample-ordered v6 plans
@@ -697,7 +646,6 @@ class GrogGridder:
         self.terms = 3 if mode == "tc" else 1
         self.n_outer = nsteps
         self.fwd6 = None
-        self.pairs = False
         dev = target_idx.device
         kwt = dict(brick=chosen, n_outer=nsteps, sub_cap=cap, n_cta=_sm_count(dev) * max(bps, 1), sample_order=True,
                    full_subs=True)
@@ -723,13 +671,13 @@ class GrogGridder:
             return "grog_grid_tc_kernel", "grog_degrid_tc_kernel"
         if m == "v8":
             return ("grog_grid_v6_kernel" if self.fwd6 is not None else "grog_grid_v8_kernel", "grog_degrid_v8_kernel")
-        k = {"v6": "v6_kernel", "v5": "v5_kernel", "v3": "v3_kernel", "global": "kernel"}.get(m, "factored_kernel")
+        k = {"v6": "v6_kernel", "global": "kernel"}[m]
         return f"grog_grid_{k}", f"grog_degrid_{k}"
 
     def launches_per_call(self, adjoint: bool) -> int:
         bp = self.plan
         if adjoint:
-            if self.mode in ("v3", "v5", "v6", "v8", "tc", "tc1"):
+            if self.mode in ("v6", "v8", "tc", "tc1"):
                 return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
             return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
         if self.mode in ("v6", "v8", "tc", "tc1"):
@@ -755,20 +703,15 @@ class GrogGridder:
             _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
                       self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
         elif self.mode == "v8":
-            _lib.call("pgb_grog_grid_v9" if self.pairs else "pgb_grog_grid_v8", data.data_ptr(), N, out.data_ptr(), G,
-                      self.inner.data_ptr(),
+            _lib.call("pgb_grog_grid_v8", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
                       self.inner.shape[0], self._outer_ptr(False), self.n_outer, C, B, _ctypes_ref(bp._c), st)
         elif self.mode == "v6":
             olc = self.outer_lc.data_ptr() if self.outer_lc is not None else None
             _lib.call("pgb_grog_grid_v6", data.data_ptr(), N, out.data_ptr(), G, self.inner_lc.data_ptr(),
                       self.inner.shape[0], olc, self.n_outer, C, B, _ctypes_ref(bp._c), st)
-        elif self.mode == "global":
+        else:
             _lib.call("pgb_grog_grid", data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(),
                       self.inner.shape[0], C, B, _ctypes_ref(bp._c_all), st)
-        else:
-            fn = {"v3": "pgb_grog_grid_v3", "v5": "pgb_grog_grid_v5"}.get(self.mode, "pgb_grog_grid_factored")
-            _lib.call(fn, data.data_ptr(), N, out.data_ptr(), G, self.inner.data_ptr(), self.inner.shape[0],
-                      self._outer_ptr(False), self.n_outer, C, B, _ctypes_ref(bp._c_all), st)
         return out
 
     def adjoint(self, grid: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
@@ -786,8 +729,7 @@ class GrogGridder:
                       int(bp.zero_src.numel()), st)
         elif self.mode == "v8":
             sec = _ctypes_ref(self.plan2._c) if self.plan2 is not None else None
-            _lib.call("pgb_grog_degrid_v9" if self.pairs else "pgb_grog_degrid_v8", grid.data_ptr(), G,
-                      out.data_ptr(), N, self.inner_h.data_ptr(),
+            _lib.call("pgb_grog_degrid_v8", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
                       self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,
                       _ctypes_ref(bp._c), sec, zs, int(bp.zero_src.numel()), st)
         elif self.mode == "v6":
@@ -796,19 +738,10 @@ class GrogGridder:
             _lib.call("pgb_grog_degrid_v6", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h_lc.data_ptr(),
                       self.inner_h.shape[0], olc, self.n_outer, C, B,
                       _ctypes_ref(bp._c), sec, zs, int(bp.zero_src.numel()), st)
-        elif self.mode in ("v3", "v5"):
-            sec = _ctypes_ref(self.plan2._c_nonempty) if self.plan2 is not None else None
-            _lib.call("pgb_grog_degrid_v3" if self.mode == "v3" else "pgb_grog_degrid_v5", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
-                      self.inner_h.shape[0], self._outer_ptr(True), self.n_outer, C, B,
-                      _ctypes_ref(bp._c_nonempty), sec, zs, int(bp.zero_src.numel()), st)
-        elif self.mode == "global":
+        else:
             _lib.call("pgb_grog_degrid", grid.data_ptr(), G, out.data_ptr(), N, self.inner_h.data_ptr(),
                       self.inner_h.shape[0], C, B, _ctypes_ref(bp._c_nonempty), 1 if bp.multi else 0,
                       zs, int(bp.zero_src.numel()), st)
-        else:
-            _lib.call("pgb_grog_degrid_factored", grid.data_ptr(), G, out.data_ptr(), N,
-                      self.inner_h.data_ptr(), self.inner_h.shape[0], self._outer_ptr(True), self.n_outer,
-                      C, B, _ctypes_ref(bp._c_nonempty), 1 if bp.multi else 0, zs, int(bp.zero_src.numel()), st)
         return out
 
 

@@ -315,249 +315,6 @@ __global__ void __launch_bounds__(kThreads) grog_expand_kernel(
   }
 }
 
-// ---------------------------------------------------------------------------
-// Factored-table kernels: T[e] = outer[e % n_outer] @ inner[e / n_outer].
-// `inner` is staged once per CTA in shared memory (persistent CTAs loop over
-// work items); `outer` rows are held in registers and applied once per run
-// of replicas sharing (outer index, cell) -- replicas inside a brick are
-// sorted by (e % n_outer, cell).  OUTER = false means T = inner (one stage).
-// ---------------------------------------------------------------------------
-constexpr int kPThreads = 512;
-constexpr int kPWarps = kPThreads / 32;
-
-template <int C>
-__device__ __forceinline__ void load_row_any(const float2* __restrict__ row, float2 (&t)[C]) {
-  if constexpr ((C % 2) == 0) {
-    const float4* r4 = reinterpret_cast<const float4*>(row);
-#pragma unroll
-    for (int i = 0; i < C / 2; ++i) {
-      const float4 v = r4[i];
-      t[2 * i] = make_float2(v.x, v.y);
-      t[2 * i + 1] = make_float2(v.z, v.w);
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < C; ++i) t[i] = row[i];
-  }
-}
-
-__device__ __forceinline__ void copy_to_smem(float2* __restrict__ dst, const float2* __restrict__ src,
-                                             int64_t n) {
-  for (int64_t t = threadIdx.x; t < n; t += blockDim.x) dst[t] = __ldg(src + t);
-}
-
-template <int C, bool OUTER>
-__global__ void __launch_bounds__(kPThreads, 1) grog_grid_factored_kernel(
-    const float2* __restrict__ data, int64_t N, float2* __restrict__ grid, int64_t G,
-    const float2* __restrict__ inner, int n_inner, const float2* __restrict__ outer, int n_outer,
-    const int32_t* __restrict__ rep_src, const uint32_t* __restrict__ rep_meta,
-    const float* __restrict__ rep_w, const int4* __restrict__ work, int n_work, BrickGeom geom) {
-  constexpr int S = 32 / C;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  const int cells = geom.bz * geom.by * geom.bx;
-  const int TS = cells + 1;
-  float2* inner_s = smem;                                   // (n_inner, C, C)
-  float2* tile = inner_s + static_cast<int64_t>(n_inner) * C * C;  // (C, TS)
-  float2* xs = tile + C * TS;                               // (warps, 32)
-  float2* us = xs + kPWarps * 32;                           // (warps, 32)
-  copy_to_smem(inner_s, inner, static_cast<int64_t>(n_inner) * C * C);
-  const int b = blockIdx.y;
-  const float2* dat = data + static_cast<int64_t>(b) * C * N;
-  float2* grd = grid + static_cast<int64_t>(b) * C * G;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int slot = lane / C;
-  const int co = lane - slot * C;
-  const unsigned smask = ((C == 32) ? 0xffffffffu : ((1u << C) - 1u)) << ((slot < S ? slot : 0) * C);
-  float2* mysx = xs + warp * 32 + slot * C;
-  float2* mysu = us + warp * 32 + slot * C;
-  __syncthreads();
-
-  for (int it = blockIdx.x; it < n_work; it += gridDim.x) {
-    const int4 item = work[it];
-    const int brick = item.x, begin = item.y, end = item.z, split = item.w;
-    for (int t = threadIdx.x; t < C * TS; t += kPThreads) tile[t] = make_float2(0.f, 0.f);
-    __syncthreads();
-    if (end > begin && slot < S) {
-      const int gslot = warp * S + slot;
-      const int nslots = kPWarps * S;
-      const int len = end - begin;
-      const int p0 = begin + static_cast<int>((static_cast<int64_t>(len) * gslot) / nslots);
-      const int p1 = begin + static_cast<int>((static_cast<int64_t>(len) * (gslot + 1)) / nslots);
-      int cur_cell = -1, cur_k = OUTER ? -1 : 0;
-      float2 acc = make_float2(0.f, 0.f);
-      float2 orow[C];
-#pragma unroll
-      for (int i = 0; i < C; ++i) orow[i] = make_float2(0.f, 0.f);
-      for (int r = p0; r <= p1; ++r) {
-        int src = 0, e = 0, cell = -1;
-        float w = 0.f;
-        bool ok = false;
-        if (r < p1) {
-          src = __ldg(rep_src + r);
-          const uint32_t meta = __ldg(rep_meta + r);
-          w = __ldg(rep_w + r);
-          e = static_cast<int>(meta & 0xFFFFFu);
-          cell = static_cast<int>(meta >> 20);
-          ok = src >= 0 && src < N && cell < cells && e < n_inner * (OUTER ? n_outer : 1);
-        }
-        const int k = OUTER ? (ok ? e % n_outer : -1) : 0;
-        const int ii = OUTER ? (ok ? e / n_outer : 0) : e;
-        // flush the running sum when the (outer index, cell) run ends
-        if (cur_cell >= 0 && (!ok || cell != cur_cell || k != cur_k)) {
-          float2 y = acc;
-          if constexpr (OUTER) {
-            __syncwarp(smask);
-            mysu[co] = acc;
-            __syncwarp(smask);
-            y = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int ci = 0; ci < C; ++ci) cfma(y, orow[ci], mysu[ci]);
-          }
-          atomicAdd(&tile[co * TS + cur_cell].x, y.x);
-          atomicAdd(&tile[co * TS + cur_cell].y, y.y);
-          cur_cell = -1;
-        }
-        if (!ok) continue;
-        if (cur_cell < 0) {
-          if (OUTER && k != cur_k) {
-            load_row<C>(outer + (static_cast<int64_t>(k) * C + co) * C, orow);
-            cur_k = k;
-          }
-          cur_cell = cell;
-          acc = make_float2(0.f, 0.f);
-        }
-        const float2 xo = __ldg(dat + static_cast<int64_t>(co) * N + src);
-        __syncwarp(smask);
-        mysx[co] = xo;
-        __syncwarp(smask);
-        float2 irow[C];
-        load_row_any<C>(inner_s + (static_cast<int64_t>(ii) * C + co) * C, irow);
-        float2 u = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int ci = 0; ci < C; ++ci) cfma(u, irow[ci], mysx[ci]);
-        acc.x = fmaf(w, u.x, acc.x);
-        acc.y = fmaf(w, u.y, acc.y);
-      }
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < C * cells; t += kPThreads) {
-      const int c = t / cells;
-      const int cl = t - c * cells;
-      int64_t flat;
-      if (!brick_cell_to_flat(geom, brick, cl, flat)) continue;
-      const float2 v = tile[c * TS + cl];
-      float2* dst = grd + static_cast<int64_t>(c) * G + flat;
-      if (split) {
-        if (v.x != 0.f || v.y != 0.f) {
-          atomicAdd(&dst->x, v.x);
-          atomicAdd(&dst->y, v.y);
-        }
-      } else {
-        *dst = v;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-template <int C, bool OUTER>
-__global__ void __launch_bounds__(kPThreads, 1) grog_degrid_factored_kernel(
-    const float2* __restrict__ grid, int64_t G, float2* __restrict__ out, int64_t N,
-    const float2* __restrict__ inner_h, int n_inner, const float2* __restrict__ outer_h, int n_outer,
-    const int32_t* __restrict__ rep_src, const uint32_t* __restrict__ rep_meta,
-    const float* __restrict__ rep_w, const int4* __restrict__ work, int n_work, BrickGeom geom,
-    int accumulate) {
-  constexpr int S = 32 / C;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  const int cells = geom.bz * geom.by * geom.bx;
-  const int TS = cells + 1;
-  float2* inner_s = smem;
-  float2* tile = inner_s + static_cast<int64_t>(n_inner) * C * C;
-  float2* vs = tile + C * TS;
-  copy_to_smem(inner_s, inner_h, static_cast<int64_t>(n_inner) * C * C);
-  const int b = blockIdx.y;
-  const float2* grd = grid + static_cast<int64_t>(b) * C * G;
-  float2* o = out + static_cast<int64_t>(b) * C * N;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int slot = lane / C;
-  const int ci = lane - slot * C;
-  const unsigned smask = ((C == 32) ? 0xffffffffu : ((1u << C) - 1u)) << ((slot < S ? slot : 0) * C);
-  float2* mysv = vs + warp * 32 + slot * C;
-  __syncthreads();
-
-  for (int it = blockIdx.x; it < n_work; it += gridDim.x) {
-    const int4 item = work[it];
-    const int brick = item.x, begin = item.y, end = item.z;
-    if (end <= begin) continue;  // block-uniform
-    for (int t = threadIdx.x; t < C * cells; t += kPThreads) {
-      const int c = t / cells;
-      const int cl = t - c * cells;
-      int64_t flat;
-      float2 v = make_float2(0.f, 0.f);
-      if (brick_cell_to_flat(geom, brick, cl, flat)) v = grd[static_cast<int64_t>(c) * G + flat];
-      tile[c * TS + cl] = v;
-    }
-    __syncthreads();
-    if (slot < S) {
-      const int gslot = warp * S + slot;
-      const int nslots = kPWarps * S;
-      const int len = end - begin;
-      const int p0 = begin + static_cast<int>((static_cast<int64_t>(len) * gslot) / nslots);
-      const int p1 = begin + static_cast<int>((static_cast<int64_t>(len) * (gslot + 1)) / nslots);
-      int cur_cell = -1, cur_k = -1;
-      float2 orow[C];
-#pragma unroll
-      for (int i = 0; i < C; ++i) orow[i] = make_float2(0.f, 0.f);
-      for (int r = p0; r < p1; ++r) {
-        const int src = __ldg(rep_src + r);
-        const uint32_t meta = __ldg(rep_meta + r);
-        const float w = __ldg(rep_w + r);
-        const int e = static_cast<int>(meta & 0xFFFFFu);
-        const int cell = static_cast<int>(meta >> 20);
-        if (!(src >= 0 && src < N && cell < cells && e < n_inner * (OUTER ? n_outer : 1))) continue;
-        const int k = OUTER ? e % n_outer : 0;
-        const int ii = OUTER ? e / n_outer : e;
-        if constexpr (OUTER) {
-          if (k != cur_k || cell != cur_cell) {
-            if (k != cur_k) {
-              load_row<C>(outer_h + (static_cast<int64_t>(k) * C + ci) * C, orow);
-              cur_k = k;
-            }
-            float2 v = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int co = 0; co < C; ++co) cfma(v, orow[co], tile[co * TS + cell]);
-            __syncwarp(smask);
-            mysv[ci] = v;
-            __syncwarp(smask);
-            cur_cell = cell;
-          }
-        }
-        float2 irow[C];
-        load_row_any<C>(inner_s + (static_cast<int64_t>(ii) * C + ci) * C, irow);
-        float2 y = make_float2(0.f, 0.f);
-        if constexpr (OUTER) {
-#pragma unroll
-          for (int co = 0; co < C; ++co) cfma(y, irow[co], mysv[co]);
-        } else {
-#pragma unroll
-          for (int co = 0; co < C; ++co) cfma(y, irow[co], tile[co * TS + cell]);
-        }
-        const float2 v = make_float2(w * y.x, w * y.y);
-        float2* dst = o + static_cast<int64_t>(ci) * N + src;
-        if (accumulate) {
-          atomicAdd(&dst->x, v.x);
-          atomicAdd(&dst->y, v.y);
-        } else {
-          *dst = v;
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
 #define PGB_FOR_EACH_C(X) \
   X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) \
   X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
@@ -580,137 +337,11 @@ static int check_geom(const pgb_brick_plan* p, BrickGeom& g, const char* who) {
 }
 
 
-size_t factored_smem_bytes(int64_t C, int cells, int64_t n_inner) {
-  return (static_cast<size_t>(n_inner) * C * C + static_cast<size_t>(C) * (cells + 1) +
-          2 * kPWarps * 32) * sizeof(float2);
-}
-
 }  // namespace pgb
 
 using namespace pgb;
 
 extern "C" {
-
-size_t pgb_grog_factored_smem_bytes(int64_t C, int64_t cells, int64_t n_inner) {
-  return factored_smem_bytes(C, static_cast<int>(cells), n_inner);
-}
-
-int pgb_grog_grid_factored(const void* data, int64_t N, void* grid, int64_t G, const void* inner,
-                           int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
-                           const pgb_brick_plan* plan, void* stream) {
-  clear_error();
-  BrickGeom geom;
-  int st = check_geom(plan, geom, "grog_grid_factored");
-  if (st) return st;
-  PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED,
-              "grog_grid_factored: ncoils must be 1..32, got %lld", (long long)C);
-  PGB_REQUIRE(N >= 0 && B >= 0 && n_inner >= 1 && n_outer >= 1 &&
-                  n_inner * n_outer <= (int64_t(1) << 20),
-              PGB_ERR_RANGE, "grog_grid_factored: invalid N/B/table sizes");
-  PGB_REQUIRE(n_outer == 1 || outer != nullptr, PGB_ERR_INVALID, "grog_grid_factored: null outer table");
-  PGB_REQUIRE(G == static_cast<int64_t>(plan->gz) * plan->gy * plan->gx, PGB_ERR_INVALID,
-              "grog_grid_factored: G does not match the plan grid");
-  PGB_REQUIRE(N < (int64_t(1) << 31), PGB_ERR_RANGE, "grog_grid_factored: N must be < 2^31");
-  if (B == 0 || G == 0) return PGB_OK;
-  PGB_REQUIRE(grid && inner && (data || N == 0), PGB_ERR_INVALID, "grog_grid_factored: null pointer");
-  PGB_REQUIRE(B <= 65535, PGB_ERR_RANGE, "grog_grid_factored: batch must be <= 65535");
-  const int cells = plan->bz * plan->by * plan->bx;
-  const size_t smem = factored_smem_bytes(C, cells, n_inner);
-  PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED,
-              "grog_grid_factored: inner table + tile need %zu B of shared memory", smem);
-  cudaStream_t s = as_stream(stream);
-  if (plan->n_split_bricks > 0) {
-    PGB_REQUIRE(plan->split_bricks != nullptr, PGB_ERR_INVALID, "grog_grid_factored: null split list");
-    const int64_t tot = static_cast<int64_t>(plan->n_split_bricks) * cells;
-    zero_bricks_kernel<<<grid_for(tot, 256, 148 * 16), 256, 0, s>>>(
-        static_cast<float2*>(grid), G, static_cast<int>(C), static_cast<int>(B), plan->split_bricks,
-        plan->n_split_bricks, geom);
-    PGB_LAUNCH_CHECK("grog_grid_factored(zero split bricks)");
-  }
-  if (plan->n_work == 0) return PGB_OK;
-  const int nblk = plan->n_work < kNumSMs ? plan->n_work : kNumSMs;
-  dim3 grd(nblk, static_cast<unsigned>(B));
-  const bool has_outer = n_outer > 1;
-  switch (C) {
-#define X(CC)                                                                                    \
-  case CC: {                                                                                     \
-    auto k = has_outer ? grog_grid_factored_kernel<CC, true> : grog_grid_factored_kernel<CC, false>; \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
-    k<<<grd, kPThreads, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), \
-                                   G, static_cast<const float2*>(inner), static_cast<int>(n_inner), \
-                                   static_cast<const float2*>(outer), static_cast<int>(n_outer),  \
-                                   plan->rep_src, plan->rep_meta, plan->rep_w,                   \
-                                   reinterpret_cast<const int4*>(plan->work), plan->n_work, geom); \
-  } break;
-    PGB_FOR_EACH_C(X)
-#undef X
-    default:
-      break;
-  }
-  PGB_LAUNCH_CHECK("grog_grid_factored");
-  return PGB_OK;
-}
-
-int pgb_grog_degrid_factored(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h,
-                             int64_t n_inner, const void* outer_h, int64_t n_outer, int64_t C,
-                             int64_t B, const pgb_brick_plan* plan, int accumulate,
-                             const int32_t* zero_src, int64_t n_zero, void* stream) {
-  clear_error();
-  BrickGeom geom;
-  int st = check_geom(plan, geom, "grog_degrid_factored");
-  if (st) return st;
-  PGB_REQUIRE(C >= 1 && C <= 32, PGB_ERR_UNSUPPORTED,
-              "grog_degrid_factored: ncoils must be 1..32, got %lld", (long long)C);
-  PGB_REQUIRE(N >= 0 && B >= 0 && n_inner >= 1 && n_outer >= 1 && n_zero >= 0 &&
-                  n_inner * n_outer <= (int64_t(1) << 20),
-              PGB_ERR_RANGE, "grog_degrid_factored: invalid N/B/table sizes");
-  PGB_REQUIRE(n_outer == 1 || outer_h != nullptr, PGB_ERR_INVALID,
-              "grog_degrid_factored: null outer table");
-  PGB_REQUIRE(G == static_cast<int64_t>(plan->gz) * plan->gy * plan->gx, PGB_ERR_INVALID,
-              "grog_degrid_factored: G does not match the plan grid");
-  PGB_REQUIRE(N < (int64_t(1) << 31), PGB_ERR_RANGE, "grog_degrid_factored: N must be < 2^31");
-  if (B == 0 || N == 0) return PGB_OK;
-  PGB_REQUIRE(out && inner_h && (grid || G == 0), PGB_ERR_INVALID, "grog_degrid_factored: null pointer");
-  PGB_REQUIRE(B <= 65535, PGB_ERR_RANGE, "grog_degrid_factored: batch must be <= 65535");
-  const int cells = plan->bz * plan->by * plan->bx;
-  const size_t smem = factored_smem_bytes(C, cells, n_inner);
-  PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED,
-              "grog_degrid_factored: inner table + tile need %zu B of shared memory", smem);
-  cudaStream_t s = as_stream(stream);
-  if (accumulate) {
-    cudaError_t e = cudaMemsetAsync(out, 0, static_cast<size_t>(B * C * N) * sizeof(float2), s);
-    PGB_REQUIRE(e == cudaSuccess, PGB_ERR_CUDA, "grog_degrid_factored: memset failed: %s",
-                cudaGetErrorString(e));
-  } else if (n_zero > 0) {
-    PGB_REQUIRE(zero_src != nullptr, PGB_ERR_INVALID, "grog_degrid_factored: null zero list");
-    zero_samples_kernel<<<grid_for(n_zero * C * B, 256, 148 * 8), 256, 0, s>>>(
-        static_cast<float2*>(out), N, static_cast<int>(C), static_cast<int>(B), zero_src, n_zero);
-    PGB_LAUNCH_CHECK("grog_degrid_factored(zero samples)");
-  }
-  if (plan->n_work == 0) return PGB_OK;
-  const int nblk = plan->n_work < kNumSMs ? plan->n_work : kNumSMs;
-  dim3 grd(nblk, static_cast<unsigned>(B));
-  const bool has_outer = n_outer > 1;
-  switch (C) {
-#define X(CC)                                                                                      \
-  case CC: {                                                                                       \
-    auto k = has_outer ? grog_degrid_factored_kernel<CC, true> : grog_degrid_factored_kernel<CC, false>; \
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);               \
-    k<<<grd, kPThreads, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N, \
-                                   static_cast<const float2*>(inner_h), static_cast<int>(n_inner), \
-                                   static_cast<const float2*>(outer_h), static_cast<int>(n_outer), \
-                                   plan->rep_src, plan->rep_meta, plan->rep_w,                     \
-                                   reinterpret_cast<const int4*>(plan->work), plan->n_work, geom,  \
-                                   accumulate);                                                    \
-  } break;
-    PGB_FOR_EACH_C(X)
-#undef X
-    default:
-      break;
-  }
-  PGB_LAUNCH_CHECK("grog_degrid_factored");
-  return PGB_OK;
-}
 
 int pgb_grog_grid(const void* data, int64_t N, void* grid, int64_t G, const void* table, int64_t K,
                   int64_t C, int64_t B, const pgb_brick_plan* plan, void* stream) {

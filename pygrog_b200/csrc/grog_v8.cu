@@ -655,8 +655,8 @@ size_t pgb_grog_v8_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t
 
 namespace {
 
-// Shared by the one-thread (v8, NT = 256) and two-thread-per-replica (v9,
-// NT = 512, even C) launches; `who` names the entry point in errors.
+// `nt` threads per CTA (kT8: one thread per replica); `who` names the entry
+// point in errors.
 int grid_v8_launch(int nt, const char* who, const void* data, int64_t N, void* grid, int64_t G,
                    const void* inner, int64_t n_inner, const void* outer, int64_t n_outer, int64_t C, int64_t B,
                    const pgb_v6_plan* plan, void* stream) {
@@ -694,9 +694,6 @@ int grid_v8_launch(int nt, const char* who, const void* data, int64_t N, void* g
 #define X(CC)                                                                                                 \
   case CC: {                                                                                                  \
     auto k = has_outer ? grog_grid_v8_kernel<CC, true, kT8> : grog_grid_v8_kernel<CC, false, kT8>;            \
-    if constexpr (CC % 2 == 0) {                                                                              \
-      if (nt != kT8) k = has_outer ? grog_grid_v8_kernel<CC, true, 2 * kT8> : grog_grid_v8_kernel<CC, false, 2 * kT8>; \
-    }                                                                                                         \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                          \
     k<<<grd, nt, smem, s>>>(static_cast<const float2*>(data), N, static_cast<float2*>(grid), G,                \
                             static_cast<const float2*>(inner), static_cast<int>(n_inner),                     \
@@ -724,15 +721,6 @@ int pgb_grog_grid_v8(const void* data, int64_t N, void* grid, int64_t G, const v
   clear_error();
   return grid_v8_launch(kT8, "grog_grid_v8", data, N, grid, G, inner, n_inner, outer, n_outer, C, B, plan, stream);
 }
-
-int pgb_grog_grid_v9(const void* data, int64_t N, void* grid, int64_t G, const void* inner, int64_t n_inner,
-                     const void* outer, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* plan,
-                     void* stream) {
-  clear_error();
-  return grid_v8_launch(2 * kT8, "grog_grid_v9", data, N, grid, G, inner, n_inner, outer, n_outer, C, B, plan,
-                        stream);
-}
-
 
 }  // extern "C"
 
@@ -784,11 +772,6 @@ int degrid_v8_launch(int nt, const char* who, const void* grid, int64_t G, void*
   case CC: {                                                                                                  \
     auto k = has_outer ? (pass ? grog_degrid_v8_kernel<CC, true, true, kT8> : grog_degrid_v8_kernel<CC, true, false, kT8>) \
                        : (pass ? grog_degrid_v8_kernel<CC, false, true, kT8> : grog_degrid_v8_kernel<CC, false, false, kT8>); \
-    if constexpr (CC % 2 == 0) {                                                                              \
-      if (nt != kT8)                                                                                          \
-        k = has_outer ? (pass ? grog_degrid_v8_kernel<CC, true, true, 2 * kT8> : grog_degrid_v8_kernel<CC, true, false, 2 * kT8>) \
-                      : (pass ? grog_degrid_v8_kernel<CC, false, true, 2 * kT8> : grog_degrid_v8_kernel<CC, false, false, 2 * kT8>); \
-    }                                                                                                         \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                          \
     k<<<grd, nt, smem, s>>>(static_cast<const float2*>(grid), G, static_cast<float2*>(out), N,                 \
                             static_cast<const float2*>(inner_h), static_cast<int>(n_inner),                   \
@@ -817,14 +800,6 @@ int pgb_grog_degrid_v8(const void* grid, int64_t G, void* out, int64_t N, const 
   clear_error();
   return degrid_v8_launch(kT8, "grog_degrid_v8", grid, G, out, N, inner_h, n_inner, outer_h, n_outer, C, B, primary,
                           secondary, zero_src, n_zero, stream);
-}
-
-int pgb_grog_degrid_v9(const void* grid, int64_t G, void* out, int64_t N, const void* inner_h, int64_t n_inner,
-                       const void* outer_h, int64_t n_outer, int64_t C, int64_t B, const pgb_v6_plan* primary,
-                       const pgb_v6_plan* secondary, const int32_t* zero_src, int64_t n_zero, void* stream) {
-  clear_error();
-  return degrid_v8_launch(2 * kT8, "grog_degrid_v9", grid, G, out, N, inner_h, n_inner, outer_h, n_outer, C, B,
-                          primary, secondary, zero_src, n_zero, stream);
 }
 
 }  // extern "C"
