@@ -65,6 +65,14 @@ class ReferenceCPU:
         self.t_inv = t.from_numpy(self.fplan["inv_perm"])
         self.t_prew = self.t_sqw[self.t_inv]
 
+    def use_table(self, table: np.ndarray) -> None:
+        """Run the reference kernels with ``table`` (K, C, C) instead of the
+        oracle's own fit (isolates the gridding path from the table fit)."""
+        t = self.torch
+        self.table = np.ascontiguousarray(table)
+        self.t_tab = t.from_numpy(self.table)
+        self.t_tabh = t.from_numpy(np.ascontiguousarray(np.conj(np.swapaxes(self.table, -1, -2))))
+
     def _interpolate(self, data: np.ndarray):
         """calib/_grog.py:668-695: replicate every sample kw times, shift each
         replica by its table entry (``grog_interpolate``), back to (C, N kw)."""

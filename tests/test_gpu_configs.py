@@ -4,7 +4,8 @@ c0  256^2 golden-angle radial, 64 spokes x 512 samples, 8 coils, 5x5 square
     kernel, oversampling 1, table precision 2, k-space = FP64 NDFT of a seeded
     ellipse phantom times Gaussian coil maps plus noise at 30 dB.  Plan keys
     (``target_idx``) and quantised shift indices bit-exact against the oracle
-    plan; ``interpolate``, ``interpolate(grid=True)`` and ``degrid`` within
+    plan; the table fit within 1e-8 of the oracle's in FP64; with the same
+    table, ``interpolate``, ``interpolate(grid=True)`` and ``degrid`` within
     1e-5 (relative L2) of the reference's own compiled CPU kernels
     (``oracle/_ref``, driven in the reference's call order by
     ``oracle/ref_cpu.py``: ``calib/_grog.py:437-555, 668-695, 736-902``).
@@ -46,9 +47,17 @@ def test_config0_matches_reference_cpu_path(cuda):
                          kernel_shape=w.kernel_shape, device=cuda)
     assert tuple(g.plan.grid_shape) == (256, 256) and int(g.plan.target_idx.shape[-1]) == 25
     np.testing.assert_array_equal(g.plan.target_idx.cpu().numpy(), ref.plan["target_idx"])
+    # table fit: the 101^2 expm powers of this calibration amplify FP32
+    # rounding (both FP32 fits differ by ~1e-3), so the fit is pinned in FP64
+    g64 = GrogInterpolator(shape=w.shape, coords=w.coords, oversamp=w.oversamp, kernel_width=w.kernel_width,
+                           kernel_shape=w.kernel_shape, device=cuda)
+    g64.calc_interp_table(w.acr.astype(np.complex128), lamda=w.lamda, precision=w.precision)
+    tab64, _, _ = og.kernel_table(w.acr.astype(np.complex128), 0.5, w.precision, w.lamda)
+    assert rel_l2(g64._interp_kernel.numpy(), tab64) < 1e-8
     g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)
     np.testing.assert_array_equal(g._interp_idx.cpu().numpy(), ref.interp_idx)
-    assert rel_l2(g._interp_kernel.numpy(), ref.table) < 1e-5
+    assert rel_l2(g._interp_kernel.numpy(), ref.table) < 1e-2
+    ref.use_table(g._interp_kernel.numpy())  # the gridding path on identical tables
 
     flat = w.data.reshape(C, -1)
     sp = g.interpolate(w.data)
