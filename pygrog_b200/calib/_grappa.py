@@ -58,6 +58,19 @@ def _logm(A: torch.Tensor) -> torch.Tensor:
     return (vecs @ torch.diag_embed(torch.log(vals)) @ torch.linalg.inv(vecs)).to(out_dtype)
 
 
+def grappa_power_device(G_unit: torch.Tensor, exponents: torch.Tensor) -> torch.Tensor:
+    """``G_unit ** e`` for each exponent in complex128 on ``G_unit``'s device:
+    ``expm(e logm(G))`` as in ``calib/_grappa.py:184-208``.  The logarithm
+    is the eigendecomposition form of :func:`_logm` (complex128), evaluated
+    on the host: there is no eigensolver for non-Hermitian matrices on the
+    GPU here, and the matrix is only ``C x C`` (C <= 32).  The matrix
+    exponentials of all fractional powers run batched on the device."""
+    dev = G_unit.device
+    L = _logm(G_unit.detach().to("cpu", torch.complex128)).to(dev)
+    e = torch.as_tensor(exponents, dtype=torch.float64, device=dev).to(L.dtype)
+    return torch.linalg.matrix_exp(e.view(-1, 1, 1) * L.unsqueeze(0))
+
+
 def grappa_power(G_unit: torch.Tensor, exponents: torch.Tensor) -> torch.Tensor:
     """Stack of ``G_unit ** e`` for each exponent, shape ``(len(e), C, C)``."""
     G_unit = torch.as_tensor(G_unit)
@@ -111,9 +124,9 @@ def _unit_operators_device(calib: torch.Tensor, lamda: float, device) -> list[to
         _lib.call("pgb_coil_cross_covariance", src.data_ptr(), src.data_ptr(), M, nc, g_ss.data_ptr(), st)
         _lib.call("pgb_coil_cross_covariance", src.data_ptr(), dst.data_ptr(), M, nc, g_sd.data_ptr(), st)
         # kernel: sum_m a[i, m] conj(b[j, m]); src^H src = its conjugate, likewise src^H dst
-        A = g_ss.cpu().conj() / norm2 + lamda * torch.eye(nc, dtype=torch.complex128)
-        Bm = g_sd.cpu().conj() / norm2
-        X = torch.linalg.solve(A, Bm)
+        A = g_ss.conj() / norm2 + lamda * torch.eye(nc, dtype=torch.complex128, device=dev)
+        Bm = g_sd.conj() / norm2
+        X = torch.linalg.solve(A, Bm)  # FP64 on the device
         ops.append(X.mT)
     return ops
 
@@ -191,9 +204,12 @@ def KernelTable(
     expm in that precision and casts the table back to the ACR's dtype.
     With ``return_factors`` a fourth item ``(outer, inner)`` is returned (see
     :func:`table_factors`), cast like the table.  ``fit_device`` (a CUDA
-    device) fits the unit operators in FP64 on that GPU
-    (:func:`_unit_operators_device`); the powers and the product follow in
-    FP64 on the host.
+    device) runs the fit in FP64 on that GPU: the least-squares Gram
+    matrices and solves (:func:`_unit_operators_device`), the matrix
+    exponentials of the fractional powers and the table product
+    (:func:`grappa_power_device`); only the ``C x C`` eigendecomposition
+    behind each logarithm runs on the host, and the finished table is copied
+    to the host.
     """
     t = torch.as_tensor(np.asarray(train_data)) if isinstance(train_data, np.ndarray) else torch.as_tensor(train_data)
     t = t.detach().cpu()
@@ -205,18 +221,20 @@ def KernelTable(
         t = t.to(fit_dtype)
     ops = train_grappa(t, lamda, device=fit_device)
     _, nsteps, deltas = shift_steps(radius, precision)
-    Gx = grappa_power(ops.x, deltas)
-    Gy = grappa_power(ops.y, deltas)
+    # the device fit stays in FP64 on the GPU through the powers and the product
+    power = grappa_power_device if fit_device is not None else grappa_power
+    Gx = power(ops.x, deltas)
+    Gy = power(ops.y, deltas)
     if ops.z is not None:
-        Gz = grappa_power(ops.z, deltas)
+        Gz = power(ops.z, deltas)
         ndim = 3
     else:
         Gz = None
         ndim = 2
-    table = prepare_grappa_table(Gx, Gy, Gz, nsteps, ndim).to(out_dtype)
+    table = prepare_grappa_table(Gx, Gy, Gz, nsteps, ndim).to(out_dtype).cpu()
     if return_factors:
         outer, inner = table_factors(Gx, Gy, Gz, ndim)
-        return table.numpy(), nsteps, ndim, (outer.to(out_dtype), inner.to(out_dtype))
+        return table.numpy(), nsteps, ndim, (outer.to(out_dtype).cpu(), inner.to(out_dtype).cpu())
     return table.numpy(), nsteps, ndim
 
 

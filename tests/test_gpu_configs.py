@@ -54,6 +54,11 @@ def test_config0_matches_reference_cpu_path(cuda):
     g64.calc_interp_table(w.acr.astype(np.complex128), lamda=w.lamda, precision=w.precision)
     tab64, _, _ = og.kernel_table(w.acr.astype(np.complex128), 0.5, w.precision, w.lamda)
     assert rel_l2(g64._interp_kernel.numpy(), tab64) < 1e-8
+    # the fit done entirely on the GPU in FP64 (cast to complex64 at the end)
+    from pygrog_b200.calib import _grappa
+
+    tdev, _, _ = _grappa.KernelTable(w.acr, 0.5, w.precision, w.lamda, fit_device=cuda)
+    assert rel_l2(tdev, tab64) < 1e-6
     g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)
     np.testing.assert_array_equal(g._interp_idx.cpu().numpy(), ref.interp_idx)
     assert rel_l2(g._interp_kernel.numpy(), ref.table) < 1e-2
@@ -103,6 +108,13 @@ def test_config2_cg_sense_matches_fp64(cuda):
 
     w = config2(ndft_device=cuda)
     C = w.data.shape[0]
+    # table fit in FP64 on the GPU against the host FP64 fit (nearly singular
+    # unit operators: 16 coils, lamda = 1e-3)
+    from pygrog_b200.calib import _grappa
+
+    tdev, _, _ = _grappa.KernelTable(w.acr, 0.5, w.precision, w.lamda, fit_device=cuda)
+    t64, _, _ = _grappa.KernelTable(w.acr, 0.5, w.precision, w.lamda, fit_dtype=torch.complex128)
+    assert rel_l2(tdev, t64) < 1e-6
     g = GrogInterpolator(shape=w.shape, coords=w.coords, oversamp=w.oversamp, kernel_width=w.kernel_width,
                          kernel_shape=w.kernel_shape, device=cuda)
     g.calc_interp_table(w.acr, lamda=w.lamda, precision=w.precision)

@@ -122,3 +122,35 @@ def test_subspace_requests_in_the_mix(cuda):
     ref = sub.op.solve(sparse.reshape(sub.C, *sub.natural_shape), method="cg", max_iter=sub.max_iter,
                        damp=sub.damp, tol=0.0)
     assert rel_l2(r.result.numpy(), ref.cpu().numpy()) < 1e-5
+
+
+def test_uneven_batch_graph_matches_alone(cuda):
+    """Protocols of different grid size, coil count and trajectory length
+    reconstructed as one CUDA graph (each a branch): every image equals the
+    same request reconstructed alone, and one equals an FP64 CG-SENSE; a
+    second launch with new k-space gives that k-space's reconstructions."""
+    from pygrog_b200.batch import UnevenBatch
+
+    protos = _protocols(cuda)
+    rng = np.random.default_rng(31)
+    for name, n, C, sp, ro in [("r32", 32, 8, 17, 64), ("r56", 56, 3, 40, 112)]:
+        acr = (rng.standard_normal((C, 12, 12)) + 1j * rng.standard_normal((C, 12, 12))).astype(np.complex64)
+        maps = gaussian_coils((n, n), C, rng).astype(np.complex64)
+        protos[name] = ReconProtocol(name, (n, n), radial2d(sp, ro, n / 2.0), acr, maps, oversamp=1.0,
+                                     kernel_width=2, max_iter=9, damp=1e-3, device=cuda)
+    plist = list(protos.values())
+    for p in plist:
+        p.prepare(1, 1, graphs=False)  # the single-request path used for comparison
+    batch = UnevenBatch(plist, cuda)
+    for launch in range(2):
+        data = [(rng.standard_normal(p.data_shape) + 1j * rng.standard_normal(p.data_shape)).astype(np.complex64)
+                for p in plist]
+        outs = batch.run([torch.from_numpy(d) for d in data])
+        assert batch.graph is not None
+        for p, d, o in zip(plist, data, outs):
+            alone = p.recon(torch.from_numpy(d).to(cuda).unsqueeze(0), 0)[0].cpu()
+            assert o.shape == alone.shape
+            assert rel_l2(o.numpy(), alone.numpy()) < 1e-5, p.name
+        if launch == 0:
+            ref = _fp64_recon(protos["spiral"], data[plist.index(protos["spiral"])])
+            assert rel_l2(outs[plist.index(protos["spiral"])].numpy(), ref) < 1e-4

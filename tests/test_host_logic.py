@@ -437,3 +437,20 @@ def test_tensor_core_timeout_count_raises(monkeypatch):
     counts[:] = [5]
     g.check_errors()  # no launch since the last check: the counter is not read
     assert counts == [5]
+
+
+def test_device_power_path_matches_host_powers_on_near_singular_operators():
+    """The device fit's fractional powers (host eigendecomposition logarithm,
+    batched matrix exponentials on the tensor's device) equal the host
+    path's on the nearly singular unit operators of a 16-coil calibration
+    with lamda = 1e-3 (eigenvalue moduli down to ~1e-5), where an iterative
+    square-root logarithm loses accuracy."""
+    from pygrog_b200.workloads import config2
+
+    w = config2()
+    ops = _grappa.train_grappa(torch.as_tensor(w.acr).to(torch.complex128), w.lamda)
+    d = _grappa.shift_steps(0.5, 1)[2]
+    for G in (ops.x, ops.y):
+        P = _grappa.grappa_power_device(G, d)
+        assert rel_l2(P.numpy(), _grappa.grappa_power(G, d).numpy()) < 1e-12
+        assert rel_l2(P[d.numel() - 1].numpy() @ P[d.numel() - 1].numpy(), G.numpy()) < 1e-10  # G^0.5 G^0.5
