@@ -129,12 +129,32 @@ __device__ __forceinline__ void split_bf2(float x, float y, uint32_t& hi, uint32
   lo = bf2(x - hf.x, y - hf.y);
 }
 
+// Samples move in chunks of kCS per CTA stage (all input coils), staged in
+// shared memory by 16-byte async copies kStages deep (in-flight bytes are what
+// bound this HBM pass), coil stride kCS + 4 float2 so the four coils a lane
+// quad reads fall in different banks.  Each warp computes two 8-sample tiles
+// per stage.
+constexpr int kCS = 128;     // samples per chunk (8 warps x two 8-sample tiles)
+constexpr int kStages = 3;   // chunks in flight per CTA
+constexpr int kXS = kCS + 4; // shared-memory coil stride (float2)
+
+__device__ __forceinline__ void cpa16(void* dst, const void* src, int bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src, int bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
 template <int CIP, int KT>  // CIP input coils (multiple of 8), KT 16-row tiles (8 output coils each)
-__global__ void __launch_bounds__(256) coil_compress_tc_kernel(const float2* __restrict__ data, int64_t N, int C,
-                                                               int K, int B, const float2* __restrict__ mat,
-                                                               float2* __restrict__ out) {
+__global__ void __launch_bounds__(256, 2) coil_compress_tc_kernel(const float2* __restrict__ data, int64_t N, int C,
+                                                                  int K, int B, const float2* __restrict__ mat,
+                                                                  float2* __restrict__ out) {
   constexpr int KC = CIP / 8;  // k16 chunks (8 input coils each)
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  extern __shared__ __align__(16) float2 xs_flat[];  // kStages buffers of CIP x kXS
+  auto xs = [&](int k) { return xs_flat + k * (CIP * kXS); };
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
   // A fragments of the realified matrix, heads and tails:
   // A[r][2c] = Re / Im part, A[r][2c + 1] = -Im / Re part (row r < 8: Re of out coil r, else Im)
   uint32_t ah[KT][KC][4], al[KT][KC][4];
@@ -153,42 +173,84 @@ __global__ void __launch_bounds__(256) coil_compress_tc_kernel(const float2* __r
         const float e1 = row < 8 ? -m.y : m.x;  // times x_im
         split_bf2(e0, e1, ah[T][kc][q], al[T][kc][q]);
       }
-  const int64_t tiles = (N + 7) / 8;
-  const int64_t total = static_cast<int64_t>(B) * tiles;
-  const int64_t warp_id = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t n_warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t w = warp_id; w < total; w += n_warps) {
-    const int64_t b = w / tiles;
-    const int64_t n0 = (w - b * tiles) * 8;
-    const int64_t n = n0 + g;  // this lane's sample in the B fragment
-    const float2* src = data + b * C * N;
-    uint32_t bh[KC][2], bl[KC][2];
-#pragma unroll
-    for (int kc = 0; kc < KC; ++kc)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c = 8 * kc + t + 4 * h;
-        const float2 x = (n < N && c < C) ? __ldg(src + static_cast<int64_t>(c) * N + n) : make_float2(0.f, 0.f);
-        split_bf2(x.x, x.y, bh[kc][h], bl[kc][h]);
-      }
-#pragma unroll
-    for (int T = 0; T < KT; ++T) {
-      float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-      for (int kc = 0; kc < KC; ++kc) {
-        mma16c(d, al[T][kc], bh[kc][0], bh[kc][1]);
-        mma16c(d, ah[T][kc], bl[kc][0], bl[kc][1]);
-        mma16c(d, ah[T][kc], bh[kc][0], bh[kc][1]);
-      }
-      // d[0], d[1]: Re of out coil 8T + g at samples 2t, 2t + 1; d[2], d[3]: Im
-      const int ko = 8 * T + g;
-      if (ko < K) {
-        float2* dst = out + (b * K + ko) * N + n0 + 2 * t;
-        if (n0 + 2 * t < N) dst[0] = make_float2(d[0], d[2]);
-        if (n0 + 2 * t + 1 < N) dst[1] = make_float2(d[1], d[3]);
+  const int64_t chunks_per_b = (N + kCS - 1) / kCS;
+  const int64_t n_chunks = static_cast<int64_t>(B) * chunks_per_b;
+  // 16-byte copies need even N and a 16-byte aligned base (pairs of samples)
+  const bool wide = (N & 1) == 0 && (reinterpret_cast<uintptr_t>(data) & 15) == 0;
+  const bool wide_out = (N & 1) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+  // stage chunk q (all coils) into buffer k; q >= n_chunks commits an empty group
+  auto stage = [&](int64_t q, int k) {
+    if (q < n_chunks) {
+      const int64_t b = q / chunks_per_b;
+      const int64_t n0 = (q - b * chunks_per_b) * kCS;
+      const float2* src = data + b * C * N;
+      for (int i = tid; i < CIP * (kCS / 2); i += 256) {  // (coil, sample pair)
+        const int c = i / (kCS / 2);
+        const int pr = i - c * (kCS / 2);
+        const int64_t n = n0 + 2 * pr;
+        float2* dst = xs(k) + c * kXS + 2 * pr;
+        const float2* sp = src + static_cast<int64_t>(c) * N + n;
+        const bool c_ok = c < C;
+        if (wide) {
+          cpa16(dst, c_ok && n < N ? sp : data, c_ok && n < N ? 16 : 0);  // N even: pairs never straddle N
+        } else {
+          cpa8(dst, c_ok && n < N ? sp : data, c_ok && n < N ? 8 : 0);
+          cpa8(dst + 1, c_ok && n + 1 < N ? sp + 1 : data, c_ok && n + 1 < N ? 8 : 0);
+        }
       }
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  const int64_t stride = gridDim.x;
+  int64_t q = blockIdx.x;
+  for (int j = 0; j < kStages - 1; ++j) stage(q + j * stride, j);
+  for (int it = 0; q < n_chunks; ++it, q += stride) {
+    const int k = it % kStages;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+    // chunk q complete in buffer k (every thread's copies), and every warp is
+    // done with the previous chunk, whose buffer is staged next
+    __syncthreads();
+    stage(q + (kStages - 1) * stride, (it + kStages - 1) % kStages);
+    const int64_t b = q / chunks_per_b;
+#pragma unroll 1
+    for (int tile = warp; tile < kCS / 8; tile += 8) {
+    const int64_t n0 = (q - b * chunks_per_b) * kCS + 8 * tile;  // this warp's 8-sample tile
+    if (n0 < N) {
+      const float2* x = xs(k) + 8 * tile + g;  // sample g of the tile
+      uint32_t bh[KC][2], bl[KC][2];
+#pragma unroll
+      for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float2 v = x[(8 * kc + t + 4 * h) * kXS];  // coil 8 kc + t + 4 h (zero beyond C)
+          split_bf2(v.x, v.y, bh[kc][h], bl[kc][h]);
+        }
+#pragma unroll
+      for (int T = 0; T < KT; ++T) {
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kc = 0; kc < KC; ++kc) {
+          mma16c(d, al[T][kc], bh[kc][0], bh[kc][1]);
+          mma16c(d, ah[T][kc], bl[kc][0], bl[kc][1]);
+          mma16c(d, ah[T][kc], bh[kc][0], bh[kc][1]);
+        }
+        // d[0], d[1]: Re of out coil 8T + g at samples 2t, 2t + 1; d[2], d[3]: Im
+        const int ko = 8 * T + g;
+        const int64_t n = n0 + 2 * t;
+        if (ko < K && n < N) {
+          float2* dst = out + (b * K + ko) * N + n;
+          if (wide_out && n + 1 < N) {
+            *reinterpret_cast<float4*>(dst) = make_float4(d[0], d[2], d[1], d[3]);
+          } else {
+            dst[0] = make_float2(d[0], d[2]);
+            if (n + 1 < N) dst[1] = make_float2(d[1], d[3]);
+          }
+        }
+      }
+    }
+    }
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 }  // namespace coil
@@ -259,8 +321,8 @@ int pgb_coil_compress_tc(const void* data, int64_t N, int64_t C, int64_t K, int6
   if (N == 0 || B == 0) return PGB_OK;
   PGB_REQUIRE(data && mat && out, PGB_ERR_INVALID, "%s: null pointer", who);
   cudaStream_t s = as_stream(stream);
-  const int64_t warps = B * ((N + 7) / 8);
-  const int blocks = grid_for(warps * 32, 256, 148 * 8);
+  const int64_t chunks = B * ((N + kCS - 1) / kCS);
+  const int blocks = static_cast<int>(chunks < 148 * 2 ? chunks : 148 * 2);  // persistent: two CTAs per SM
   const int cip = static_cast<int>((C + 7) / 8 * 8);
   const int kt = K > 8 ? 2 : 1;
   const float2* d = static_cast<const float2*>(data);
@@ -268,8 +330,12 @@ int pgb_coil_compress_tc(const void* data, int64_t N, int64_t C, int64_t K, int6
   float2* o = static_cast<float2*>(out);
   const int Ci = static_cast<int>(C), Ki = static_cast<int>(K), Bi = static_cast<int>(B);
   switch (cip * 10 + kt) {
-#define X(CI, KTT) \
-  case CI * 10 + KTT: coil_compress_tc_kernel<CI, KTT><<<blocks, 256, 0, s>>>(d, N, Ci, Ki, Bi, m, o); break;
+#define X(CI, KTT)                                                                                  \
+  case CI * 10 + KTT: {                                                                             \
+    const int smem = kStages * CI * kXS * static_cast<int>(sizeof(float2));                         \
+    cudaFuncSetAttribute(coil_compress_tc_kernel<CI, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
+    coil_compress_tc_kernel<CI, KTT><<<blocks, 256, smem, s>>>(d, N, Ci, Ki, Bi, m, o);              \
+  } break;
     X(8, 1) X(16, 1) X(16, 2) X(24, 1) X(24, 2) X(32, 1) X(32, 2)
 #undef X
     default:

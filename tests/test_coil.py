@@ -1,4 +1,4 @@
-"""Coil compression (SURVEY row "next": the PCA step before the GROG path).
+"""Coil compression: the PCA step before the GROG path (utils/_coil_compress.py:23-57).
 
 CPU: properties of the FP64 oracle.  GPU: the device covariance, matrix and
 compression against the oracle on the same seeded data."""
@@ -84,7 +84,8 @@ def test_gpu_coil_compress_batched_kernel(cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("C,K,B,N", [(32, 12, 1, 4099), (32, 16, 2, 1000), (12, 5, 1, 777), (20, 9, 3, 64)])
+@pytest.mark.parametrize("C,K,B,N", [(32, 12, 1, 4099), (32, 16, 2, 1000), (12, 5, 1, 777), (20, 9, 3, 64),
+                                     (32, 12, 2, 200_000), (8, 8, 1, 130)])
 def test_gpu_coil_compress_tensor_cores(cuda, C, K, B, N):
     """bf16x3 tensor-core compression within 1e-5 of the FP64 product."""
     from pygrog_b200 import _lib
