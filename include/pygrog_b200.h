@@ -148,6 +148,37 @@ PGB_API int pgb_plan_quantize(const float* distances, int64_t R, int ndim, float
                       float pfac, float stepsize, int nsteps, int64_t K,
                       int64_t* interp_idx, void* stream);
 
+/* Host-side packing steps of the brick plans of the fused gridders (host
+ * pointers, no device work; sequential per sub-chunk, threaded over
+ * sub-chunks).  No reference counterpart: the reference computes every
+ * replica unbinned (calib/_grog.py:1283-1295); these lay the binned replicas
+ * out for the kernels below.
+ *
+ * pgb_plan_pack_quarter_warps: sub-chunk s holds replicas
+ * [sub_ptr[s], sub_ptr[s + 1]) in processing order with inner / outer table
+ * indices q / k; every replica gets lane = quarter_warp * per + slot, packing
+ * nq[s] = ceil(count / per) quarter-warps first-fit: a replica goes to the
+ * first quarter-warp with a free lane that already reads its inner operator,
+ * else has its inner residue class (q mod per) free, both with a compatible
+ * outer residue (k mod per: free or the same k), else has a compatible inner
+ * residue, else has the fewest lanes taken.  per = 8 or 4.
+ *
+ * pgb_plan_pack_rows: sub-chunk s holds cell runs [run_ptr[s], run_ptr[s+1])
+ * of run_len entries; runs are laid out in order from entry 0, a run of at
+ * most `rows` entries that would cross a multiple of `rows` starts at the
+ * next one (padding entries in between) as long as the sub-chunk's entries
+ * stay within `cap`; run_start gets each run's first entry, n_entries[s] the
+ * sub-chunk's entries including padding.
+ *
+ * pgb_plan_lpt: item i of cost[i] goes to out[i] in [0, bins): items in
+ * decreasing cost (ties in index order), each to the least loaded bin (ties
+ * to the lowest bin). */
+PGB_API int pgb_plan_pack_quarter_warps(const int64_t* sub_ptr, const int64_t* q, const int64_t* k,
+                                        int64_t n_subs, int64_t per, int64_t* lane, int64_t* nq);
+PGB_API int pgb_plan_pack_rows(const int64_t* run_len, const int64_t* run_ptr, int64_t n_subs, int64_t rows,
+                               int64_t cap, int64_t* run_start, int64_t* n_entries);
+PGB_API int pgb_plan_lpt(const double* cost, int64_t n, int64_t bins, int32_t* out);
+
 /* =====================================================================
  * Fused GROG operator (interpolate + weight + scatter, and its adjoint)
  * ===================================================================== */

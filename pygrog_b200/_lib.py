@@ -125,6 +125,9 @@ _SIGS = {
     "pgb_lsmr_v_full": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_lsmr_scalars": [_vp, _vp],
     "pgb_lsmr_vec_update": [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp],
+    "pgb_plan_pack_quarter_warps": [_vp, _vp, _vp, _i64, _i64, _vp, _vp],
+    "pgb_plan_pack_rows": [_vp, _vp, _i64, _i64, _i64, _vp, _vp],
+    "pgb_plan_lpt": [_vp, _i64, _i64, _vp],
     "pgb_coil_covariance": [_vp, _i64, _i64, _vp, _vp],
     "pgb_coil_cross_covariance": [_vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_coil_compress": [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp],

@@ -213,33 +213,18 @@ class BrickPlan6:
                 # meta -1, in between) while the sub-chunk's padding budget
                 # allows; only runs longer than an m-tile still cross one
                 rsub = sub_id[head]
-                rk = torch.arange(run_len.numel(), device=dev) - (torch.cumsum(
-                    torch.bincount(rsub, minlength=n_subs), 0) - torch.bincount(rsub, minlength=n_subs))[rsub]
-                max_r = int(rk.max()) + 1
-                L2 = torch.zeros(n_subs, max_r, dtype=torch.int64, device=dev)
-                L2[rsub, rk] = run_len
-                rem = L2.flip(1).cumsum(1).flip(1)
-                cur = torch.zeros(n_subs, dtype=torch.int64, device=dev)
-                starts = torch.zeros_like(L2)
-                T = pack_rows
-                for kk in range(max_r):
-                    ln = L2[:, kk]
-                    off = cur % T
-                    pad = torch.where((ln > 0) & (ln <= T) & (off + ln > T), T - off, torch.zeros_like(off))
-                    pad = torch.where(cur + pad + rem[:, kk] <= self.sub_cap, pad, torch.zeros_like(pad))
-                    cur = cur + pad
-                    starts[:, kk] = cur
-                    cur = cur + ln
-                new_pos = starts[rsub, rk][run_id] + (pos - rs)
-                nslot = cur  # entries per sub-chunk, padding included
+                run_ptr = torch.cumsum(torch.bincount(rsub, minlength=n_subs), 0)
+                run_ptr = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), run_ptr])
+                run_start, nslot = _native_pack_rows(run_len, run_ptr, n_subs, pack_rows, self.sub_cap)
+                new_pos = run_start[run_id] + (pos - rs)  # nslot: entries per sub-chunk, padding included
                 sbase = torch.cumsum(nslot, 0) - nslot
                 total = int(nslot.sum())
                 dest = sbase[sub_id] + new_pos
                 pad = torch.ones(total, dtype=torch.bool, device=dev)
                 pad[dest] = False
-                rs = starts[rsub, rk][run_id]
+                rs = run_start[run_id]
                 re = rs + run_len[run_id] - 1
-                straddle = (rs // T) != (re // T)
+                straddle = (rs // pack_rows) != (re // pack_rows)
 
                 def spread(v, fill):
                     out = torch.full((total,), fill, dtype=v.dtype, device=dev)
@@ -373,55 +358,24 @@ def _pack_quarter_warps(sub_id: torch.Tensor, q: torch.Tensor, k: torch.Tensor, 
     quad q mod 8.  ``per = 4``: two lanes per replica reading rows 0..C/2-1 and
     C/2..C-1 (4 quads apart when C = 12, mod 8), classes q mod 4.
 
-    Replicas come grouped by sub-chunk, each group in its processing order; the
-    sub-chunks are packed side by side, one replica of each per step.  A replica
-    goes to the first quarter-warp with a free lane that (1) already reads its
-    inner operator, else (2) has its inner residue free, both with a compatible
-    outer residue, else (3) has a compatible inner residue, else (4) has the
-    fewest lanes taken.  Returns ``(lane, quarter-warps per sub-chunk)``.
+    Replicas come grouped by sub-chunk, each group in its processing order.  A
+    replica goes to the first quarter-warp with a free lane that (1) already
+    reads its inner operator, else (2) has its inner residue free, both with a
+    compatible outer residue, else (3) has a compatible inner residue, else (4)
+    has the fewest lanes taken (native ``pgb_plan_pack_quarter_warps``, one
+    sequential pass per sub-chunk).  Returns ``(lane, quarter-warps per
+    sub-chunk)`` on the inputs' device.
     """
     dev = sub_id.device
-    n = sub_id.numel()
     cnt = torch.bincount(sub_id, minlength=n_subs)
-    nq = (cnt + per - 1) // per
-    nres = per
-    if n == 0:
-        return torch.zeros(0, dtype=torch.int64, device=dev), nq
-    nqw = int(nq.max())
-    step = torch.arange(n, device=dev) - (torch.cumsum(cnt, 0) - cnt)[sub_id]
-    order = torch.sort(step, stable=True)[1]
-    steps = torch.bincount(step)
-    used = torch.zeros(n_subs, nqw, dtype=torch.int64, device=dev)
-    used[torch.arange(nqw, device=dev)[None, :] >= nq[:, None]] = per  # quarter-warps beyond ceil(n / per)
-    res_q = torch.full((n_subs, nqw, nres), -1, dtype=torch.int64, device=dev)
-    res_k = torch.full((n_subs, nqw, nres), -1, dtype=torch.int64, device=dev)
-    lane = torch.empty(n, dtype=torch.int64, device=dev)
-    big = nqw + 1
-    col = torch.arange(nqw, device=dev)[None, :]
-    i0 = 0
-    for m in steps.tolist():
-        idx = order[i0:i0 + m]
-        i0 += m
-        sb, qq, kk = sub_id[idx], q[idx], k[idx]
-        cq = res_q[sb[:, None], col, (qq % nres)[:, None]]
-        ck = res_k[sb[:, None], col, (kk % nres)[:, None]]
-        u = used[sb]
-        free = u < per
-        ok_k = (ck < 0) | (ck == kk[:, None])
-        same_q = cq == qq[:, None]
-        cands = (free & same_q & ok_k, free & (cq < 0) & ok_k, free & ((cq < 0) | same_q))
-        pick = torch.full((m,), big, dtype=torch.int64, device=dev)
-        for c in cands:
-            first = torch.where(c, col, big).min(1).values
-            pick = torch.where(pick == big, first, pick)
-        fewest = torch.where(free, u, per + 1).argmin(1)
-        pick = torch.where(pick == big, fewest, pick)
-        lane[idx] = pick * per + u.gather(1, pick[:, None]).squeeze(1)
-        used[sb, pick] += 1
-        for res, r, v in ((res_q, qq % nres, qq), (res_k, kk % nres, kk)):
-            cur = res[sb, pick, r]
-            res[sb, pick, r] = torch.where(cur < 0, v, cur)
-    return lane, nq
+    ptr = np.concatenate([[0], np.cumsum(_host_i64(cnt))]).astype(np.int64)
+    qh, kh = _host_i64(q), _host_i64(k)
+    lane = np.zeros(qh.size, dtype=np.int64)
+    nq = np.zeros(n_subs, dtype=np.int64)
+    if n_subs:
+        _lib.call("pgb_plan_pack_quarter_warps", ptr.ctypes.data, qh.ctypes.data, kh.ctypes.data, int(n_subs),
+                  int(per), lane.ctypes.data, nq.ctypes.data)
+    return torch.from_numpy(lane).to(dev), torch.from_numpy(nq).to(dev)
 
 
 def _sm_count(dev) -> int:
@@ -431,13 +385,30 @@ def _sm_count(dev) -> int:
 
 
 def _lpt_assign(cost: np.ndarray, n_bins: int) -> np.ndarray:
-    """Longest-processing-time-first assignment of items to ``n_bins`` bins."""
-    import heapq
+    """Longest-processing-time-first assignment of items to ``n_bins`` bins
+    (largest item first, to the least loaded bin, ties to the lowest bin;
+    native ``pgb_plan_lpt``)."""
+    c = np.ascontiguousarray(cost, dtype=np.float64)
+    out = np.zeros(len(c), dtype=np.int32)
+    if len(c):
+        _lib.call("pgb_plan_lpt", c.ctypes.data, len(c), int(n_bins), out.ctypes.data)
+    return out.astype(np.int64)
 
-    out = np.zeros(len(cost), dtype=np.int64)
-    heap = [(0.0, b) for b in range(n_bins)]
-    for i in np.argsort(-cost, kind="stable"):
-        load, b = heapq.heappop(heap)
-        out[i] = b
-        heapq.heappush(heap, (load + float(cost[i]), b))
-    return out
+
+def _host_i64(t: torch.Tensor) -> np.ndarray:
+    return np.ascontiguousarray(t.detach().to("cpu", torch.int64).numpy())
+
+
+def _native_pack_rows(run_len: torch.Tensor, run_ptr: torch.Tensor, n_subs: int, rows: int, cap: int):
+    """Next-fit packing of each sub-chunk's cell runs into ``rows``-row
+    m-tiles (native ``pgb_plan_pack_rows``): a run that would cross an m-tile
+    starts the next one while the sub-chunk's ``cap`` entries allow the
+    padding.  Returns (start of every run, entries per sub-chunk) on the
+    runs' device."""
+    rl, rp = _host_i64(run_len), _host_i64(run_ptr)
+    start = np.zeros(rl.size, dtype=np.int64)
+    nent = np.zeros(max(n_subs, 0), dtype=np.int64)
+    _lib.call("pgb_plan_pack_rows", rl.ctypes.data, rp.ctypes.data, int(n_subs), int(rows), int(cap),
+              start.ctypes.data, nent.ctypes.data)
+    dev = run_len.device
+    return torch.from_numpy(start).to(dev), torch.from_numpy(nent).to(dev)
