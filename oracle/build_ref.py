@@ -43,7 +43,18 @@ def built_path() -> pathlib.Path | None:
     return None
 
 
-def build(src_root: str = "/root/reference", verbose: bool = False) -> pathlib.Path:
+# Where this recipe finds the reference checkout (its sources are compiled
+# where they lie; override with PYGROG_REFERENCE).
+DEFAULT_SRC = os.environ.get("PYGROG_REFERENCE", "/root/reference")
+
+
+def source_root() -> pathlib.Path | None:
+    """The reference checkout if its C++ sources are present, else None."""
+    root = pathlib.Path(DEFAULT_SRC)
+    return root if (root / "csrc" / "torch").exists() else None
+
+
+def build(src_root: str = DEFAULT_SRC, verbose: bool = False) -> pathlib.Path:
     import torch.utils.cpp_extension as cpp_ext
 
     csrc = pathlib.Path(src_root) / "csrc" / "torch"
@@ -96,7 +107,7 @@ def load():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=DEFAULT_SRC)
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     p = build(a.src, a.verbose)
