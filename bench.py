@@ -36,6 +36,7 @@ sys.path.insert(0, str(REPO))
 
 N_SPOKES, N_READOUT, GRID_N, N_COILS_RAW, N_COILS = 20000, 384, 192, 32, 12
 CPU_SAMPLE_SPOKES = 2000
+C3_LANES = (8, 16, 64)  # parallel chains of the c3 batch graph to time (the fastest is reported)
 METRIC = "GROG samples*coils/s fwd+adj (3-D kooshball 192^3, C=12)"
 UNIT = "samples*coils/s"
 
@@ -154,10 +155,17 @@ def build_workload(device, seed: int = 1001):
     from pygrog_b200.workloads import kooshball
 
     coords = kooshball(N_SPOKES, N_READOUT, GRID_N / 2.0)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
     g = GrogInterpolator(shape=(GRID_N,) * 3, coords=coords, oversamp=1.0, kernel_width=2,
                          kernel_shape="sphere", device=device)
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
     acr = make_acr3d(device, seed)
+    t2 = time.perf_counter()
     g.calc_interp_table(acr, lamda=0.01, precision=1)
+    torch.cuda.synchronize(device)
+    g.setup_ms = {"plan": (t1 - t0) * 1e3, "table": (time.perf_counter() - t2) * 1e3}
     gen = torch.Generator(device=device).manual_seed(seed)
     N = N_SPOKES * N_READOUT
     data = torch.randn(1, N_COILS, N, dtype=torch.complex64, device=device, generator=gen)
@@ -486,31 +494,40 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
         protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
                                      device=dev, **kw)
     t_proto = time.perf_counter() - t0
-    batch = UnevenBatch(list(protos.values()), dev)
     gen = torch.Generator().manual_seed(seed)
-    for h in batch.host_in:
-        h.copy_(torch.randn(h.shape, dtype=torch.complex64, generator=gen))
-    t1 = time.perf_counter()
-    batch.capture()
-    torch.cuda.synchronize(dev)
-    t_capture = time.perf_counter() - t1
-    walls = []
-    for _ in range(6):  # first run warms
-        t2 = time.perf_counter()
-        batch.run()
-        walls.append(time.perf_counter() - t2)
-    wall = min(walls[1:])
+    host_in = [torch.randn(p.data_shape, dtype=torch.complex64, generator=gen).pin_memory() for p in protos.values()]
+    best = None
+    by_lanes = {}
+    for lanes in C3_LANES:
+        batch = UnevenBatch(list(protos.values()), dev, lanes=lanes)
+        batch.host_in = host_in  # the caller's page-locked k-space, read by the graph's copies
+        t1 = time.perf_counter()
+        batch.capture()
+        torch.cuda.synchronize(dev)
+        t_capture = time.perf_counter() - t1
+        walls = []
+        for _ in range(6):  # first run warms
+            t2 = time.perf_counter()
+            batch.run()
+            walls.append(time.perf_counter() - t2)
+        by_lanes[str(lanes)] = min(walls[1:]) * 1e3
+        if best is None or min(walls[1:]) < best[0]:
+            best = (min(walls[1:]), lanes, t_capture)
+        del batch
+        torch.cuda.empty_cache()
+    wall, lanes_best, t_capture = best
     sc = sum(p.C * int(np.prod(p.spatial)) for p in protos.values())
     # the per-request path on 4 streams, for comparison
     server = ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=4, device=dev)
-    data = {k: h for k, h in zip(protos, batch.host_in)}
+    data = {k: h for k, h in zip(protos, host_in)}
     prev = []
     for _ in range(3):
         reqs = [Request(i, k, 0.0, data[k]) for i, k in enumerate(protos)]
         prev.append(server.run(reqs, realtime=False)["wall_s"])
-    del server, batch
+    del server
     torch.cuda.empty_cache()
-    return {"slices": n_slices, "ms_per_batch": wall * 1e3, "sample_coils": sc,
+    return {"slices": n_slices, "ms_per_batch": wall * 1e3, "lanes": lanes_best, "ms_by_lanes": by_lanes,
+            "sample_coils": sc,
             "sample_coils_per_s": sc / wall, "recons_per_s": n_slices / wall, "cg_iters": 20,
             "setup_s": t_proto + t_capture, "protocols_s": t_proto, "capture_s": t_capture,
             "per_request_streams_ms": min(prev[1:]) * 1e3, "mode": "one graph, slices as branches",
@@ -518,8 +535,13 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
 
 
 def cg_sense_c2(dev, iters: int = 30) -> dict:
-    """Time per CG-SENSE iteration of config c2 (spiral 320^2, 16 coils, Toeplitz on 640^2),
-    one CUDA graph of ``iters`` iterations, CUDA events."""
+    """Config c2 (spiral 320^2, 16 coils, Toeplitz PSF on 640^2, 30 CG
+    iterations): time per reconstruction (GROG interpolation + SparseFFT
+    adjoint + the graph-replayed CG) and per CG iteration (the captured
+    iterations alone), CUDA events; the iteration's roofline from the bytes
+    its passes move: coil expansion into the padded grid, the forward and
+    inverse 2-D FFTs (two passes each, read + write), the PSF multiply
+    (read + write), the crop + coil combine, and the CG vector updates."""
     import torch
 
     from pygrog_b200.serve import ReconProtocol
@@ -534,17 +556,71 @@ def cg_sense_c2(dev, iters: int = 30) -> dict:
         p.recon(d, 0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
-    e0.record()
     reps = 5
+    e0.record()
     for _ in range(reps):
         p.recon(d, 0)
     e1.record()
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / reps
+    cg = p._solvers[0]  # the captured CG iterations alone (state from the last recon)
+    e0.record()
+    for _ in range(reps):
+        cg.run(p.max_iter)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms_iter = e0.elapsed_time(e1) / reps / p.max_iter
     G = int(np.prod(p.op.grid_shape))
-    return {"ms_per_recon": ms, "cg_iters": p.max_iter, "coils": p.C, "grid": list(p.op.grid_shape),
-            "fft_gflop_per_iter": 2 * p.C * 5 * G * float(np.log2(G)) / 1e9,
+    img = int(np.prod(p.image_shape))
+    C = p.C
+    grid_b = C * G * 8
+    iter_bytes = (img * 8 + C * img * 8 + grid_b  # expand: x, maps in, padded coil grid out
+                  + 4 * grid_b + 2 * grid_b + G * 4 + 4 * grid_b  # FFT (2 passes), PSF (r + w, PSF), IFFT
+                  + 2 * C * img * 8 + 2 * img * 8  # crop + combine (coil images, maps), damp add
+                  + 8 * img * 8)  # CG: two FP64 dots and the x / r / p updates
+    peak, _ = _peaks()
+    gbs = iter_bytes / (ms_iter / 1e3) / 1e9
+    return {"ms_per_recon": ms, "ms_per_iter": ms_iter, "cg_iters": p.max_iter, "coils": C,
+            "grid": list(p.op.grid_shape), "iter_bytes": iter_bytes, "iter_gbs": gbs,
+            "iter_roofline_frac": gbs / peak, "fft_gflop_per_iter": 2 * C * 5 * G * float(np.log2(G)) / 1e9,
             "note": "recon = GROG interpolate + SparseFFT adjoint + graph-replayed CG (Toeplitz normal)"}
+
+
+def serve_sweep(dev, rates=(200.0, 300.0, 400.0, 600.0), seconds: float = 5.0, seed: int = 1004) -> dict:
+    """Open-loop Poisson arrivals of the c4 mix at several rates, served by the
+    batched server (8 frames per batch, 4 streams) and by the plain
+    single-instance path (one request at a time, one stream): p50 / p95 / p99
+    latency and served recons/s per rate."""
+    import torch
+
+    from pygrog_b200.serve import ReconProtocol, ReconServer, Request, poisson_arrivals
+    from pygrog_b200.workloads import serving_protocols, subspace_protocol
+
+    specs = serving_protocols(seed) + [subspace_protocol()]
+    protos = {}
+    for sp in specs:
+        kw = dict(sp)
+        name = kw.pop("name")
+        protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
+                                     device=dev, **kw)
+    names = list(protos)
+    others = [k for k in names if not protos[k].subspace]
+    prob = np.array([0.2 if protos[k].subspace else 0.8 / len(others) for k in names])
+    rng = np.random.default_rng(seed)
+    servers = {"batched": ReconServer(protos, mem_budget=150 << 30, max_batch=8, n_slots=4, device=dev),
+               "single": ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=1, device=dev)}
+    out = {}
+    for rate in rates:
+        arr = poisson_arrivals(rate, seconds, rng)
+        for kind, srv in servers.items():
+            reqs = []
+            for i, t in enumerate(arr):
+                p = protos[names[int(rng.choice(len(names), p=prob))]]
+                reqs.append(Request(i, p.name, float(t), torch.randn(p.data_shape, dtype=torch.complex64).pin_memory()))
+            rep = srv.run(reqs, realtime=True)
+            out[f"{kind}@{int(rate)}"] = {k: rep[k] for k in ("requests", "recons_per_s", "p50_ms", "p95_ms", "p99_ms",
+                                                            "mean_batch")}
+    return {"seconds_per_rate": seconds, "rates": list(rates), "results": out}
 
 
 def _call_workloads():
@@ -640,7 +716,7 @@ def _compact_sections(coilc, cg2, c3, serving, tune):
         return {k: _r(d[k]) for k in keys if k in d}
 
     out["coil_compress_c1"] = pick(coilc, ("tc_ms", "tc_gbs", "tc_frac", "fp32_ms", "tc_rel_err_vs_fp32"))
-    out["cg_sense_c2"] = pick(cg2, ("ms_per_recon", "ms_per_iter", "iter_roofline_frac"))
+    out["cg_sense_c2"] = pick(cg2, ("ms_per_recon", "ms_per_iter", "iter_gbs", "iter_roofline_frac"))
     out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "setup_s", "per_request_streams_ms"))
     if isinstance(serving, dict) and "error" not in serving:
         o = serving.get("open_loop", {})
@@ -677,6 +753,8 @@ def main():
     ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
     ap.add_argument("--calls", action="store_true",
                     help="only time the public API call by call on configs c0 and c2 (one JSON line)")
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="only sweep open-loop arrival rates of the served mix, batched vs single-instance (one JSON line)")
     ap.add_argument("--details", default=None,
                     help="also write the full per-section results (precision modes, serving, c2, c3) to this file")
     args = ap.parse_args()
@@ -702,6 +780,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.serve_sweep:
+        if rank == 0:
+            print(json.dumps({"serve_sweep": serve_sweep(dev), "device": torch.cuda.get_device_name(dev)}), flush=True)
+        return 0
     if args.calls:
         if rank == 0:
             print(json.dumps({"calls": time_calls(dev), "device": torch.cuda.get_device_name(dev),
@@ -711,7 +793,10 @@ def main():
     g, coords, acr, data = build_workload(dev)
     if args.table_mode and args.table_mode != "auto":
         g.gridder_mode = args.table_mode
+    t0 = time.perf_counter()
     bp = g._brick(0)
+    torch.cuda.synchronize(dev)
+    g.setup_ms["gridder_plans"] = (time.perf_counter() - t0) * 1e3
     G = int(np.prod(g.plan.grid_shape))
     B, C, N = data.shape
     kgrid = torch.empty(B, C, G, dtype=torch.complex64, device=dev)
@@ -876,6 +961,7 @@ def main():
             },
             "fwd_ms": fwd_ms,
             "adj_ms": adj_ms,
+            "setup_ms": {k: round(v, 1) for k, v in g.setup_ms.items()},
             "roofline": {
                 "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,

@@ -25,6 +25,7 @@ from __future__ import annotations
 __all__ = ["UnevenBatch"]
 
 import gc
+import math
 
 import torch
 
@@ -35,13 +36,14 @@ class UnevenBatch:
     """One CUDA graph reconstructing one request of each protocol in ``protocols``.
 
     ``protocols``: :class:`pygrog_b200.serve.ReconProtocol` objects (their
-    plans, tables, coil maps and PSFs resident on ``device``).  Inputs go in
+    plans, tables, coil maps and PSFs resident on ``device``).  ``lanes``:
+    number of parallel chains in the graph (default: one per protocol).  Inputs go in
     :attr:`host_in` (page-locked, one ``(C, *spatial)`` tensor per protocol),
     :meth:`run` launches the graph and returns :attr:`host_out` (page-locked
     ``image_shape`` tensors).
     """
 
-    def __init__(self, protocols, device=None):
+    def __init__(self, protocols, device=None, lanes: int | None = None):
         self.protos = list(protocols)
         if not self.protos:
             raise ValueError("UnevenBatch needs at least one protocol")
@@ -51,7 +53,19 @@ class UnevenBatch:
         self._dev_in = [torch.empty((1, *p.data_shape), dtype=torch.complex64, device=self.device)
                         for p in self.protos]
         self._cg = [BatchedDeviceCG(p.op, 1, p.image_shape, self.device, damp=p.damp, tol=0.0) for p in self.protos]
-        self._streams = [torch.cuda.Stream(self.device) for _ in self.protos]
+        # parallel chains of the graph: every slice its own branch by default;
+        # with `lanes`, the slices are dealt largest first (samples x coils x
+        # CG iterations) to the lane with the least work, each lane a chain
+        n = len(self.protos) if lanes is None else max(1, min(int(lanes), len(self.protos)))
+        cost = [p.C * max(math.prod(p.spatial), 1) * max(p.max_iter, 1) for p in self.protos]
+        load = [0.0] * n
+        self._lane_of = [0] * len(self.protos)
+        self._order = sorted(range(len(self.protos)), key=lambda j: -cost[j])  # capture order: largest first
+        for i in self._order:
+            ln = min(range(n), key=lambda k: load[k])
+            self._lane_of[i] = ln
+            load[ln] += cost[i]
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(n)]
         self.graph = None
 
     def _branch(self, i: int) -> None:
@@ -72,9 +86,10 @@ class UnevenBatch:
 
     def _all_branches(self) -> None:
         main = torch.cuda.current_stream(self.device)
-        for i, s in enumerate(self._streams):
+        for s in self._streams:
             s.wait_stream(main)
-            with torch.cuda.stream(s):
+        for i in self._order:
+            with torch.cuda.stream(self._streams[self._lane_of[i]]):
                 self._branch(i)
         for s in self._streams:
             main.wait_stream(s)
