@@ -610,13 +610,16 @@ def serve_sweep(dev, rates=(200.0, 300.0, 400.0, 600.0), seconds: float = 5.0, s
     servers = {"batched": ReconServer(protos, mem_budget=150 << 30, max_batch=8, n_slots=4, device=dev),
                "single": ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=1, device=dev)}
     out = {}
-    for rate in rates:
-        arr = poisson_arrivals(rate, seconds, rng)
-        for kind, srv in servers.items():
+    arrivals = {rate: poisson_arrivals(rate, seconds, rng) for rate in rates}
+    # one page-locked k-space per protocol, shared by its requests (timing does not depend on the values)
+    kspace = {k: torch.randn(p.data_shape, dtype=torch.complex64).pin_memory() for k, p in protos.items()}
+    for kind, srv in servers.items():
+        for rate in rates:
+            arr = arrivals[rate]
             reqs = []
             for i, t in enumerate(arr):
                 p = protos[names[int(rng.choice(len(names), p=prob))]]
-                reqs.append(Request(i, p.name, float(t), torch.randn(p.data_shape, dtype=torch.complex64).pin_memory()))
+                reqs.append(Request(i, p.name, float(t), kspace[p.name]))
             rep = srv.run(reqs, realtime=True)
             out[f"{kind}@{int(rate)}"] = {k: rep[k] for k in ("requests", "recons_per_s", "p50_ms", "p95_ms", "p99_ms",
                                                             "mean_batch")}
@@ -753,6 +756,8 @@ def main():
     ap.add_argument("--c3-slices", type=int, default=64, help="slices of the c3 batch (0: skip)")
     ap.add_argument("--calls", action="store_true",
                     help="only time the public API call by call on configs c0 and c2 (one JSON line)")
+    ap.add_argument("--coil-only", action="store_true",
+                    help="only time the coil compression (32 -> --coils) of --spokes x --readout samples (one JSON line)")
     ap.add_argument("--serve-sweep", action="store_true",
                     help="only sweep open-loop arrival rates of the served mix, batched vs single-instance (one JSON line)")
     ap.add_argument("--details", default=None,
@@ -780,6 +785,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.coil_only:
+        if rank == 0:
+            r = coil_compress_c1(dev)
+            print(json.dumps({"coil_compress": {k: v for k, v in r.items() if not isinstance(v, dict)},
+                              "samples": N_SPOKES * N_READOUT}), flush=True)
+        return 0
     if args.serve_sweep:
         if rank == 0:
             print(json.dumps({"serve_sweep": serve_sweep(dev), "device": torch.cuda.get_device_name(dev)}), flush=True)

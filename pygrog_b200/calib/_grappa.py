@@ -60,15 +60,25 @@ def _logm(A: torch.Tensor) -> torch.Tensor:
 
 def grappa_power_device(G_unit: torch.Tensor, exponents: torch.Tensor) -> torch.Tensor:
     """``G_unit ** e`` for each exponent in complex128 on ``G_unit``'s device:
-    ``expm(e logm(G))`` as in ``calib/_grappa.py:184-208``.  The logarithm
-    is the eigendecomposition form of :func:`_logm` (complex128), evaluated
-    on the host: there is no eigensolver for non-Hermitian matrices on the
-    GPU here, and the matrix is only ``C x C`` (C <= 32).  The matrix
-    exponentials of all fractional powers run batched on the device."""
+    ``expm(e logm(G))`` of ``calib/_grappa.py:184-208``, evaluated in the
+    eigenbasis of the logarithm, ``V diag(exp(e l)) V^-1`` with
+    ``logm(G) = V diag(l) V^-1`` (the eigendecomposition form of
+    :func:`_logm`).  The ``C x C`` eigendecomposition (complex128, C <= 32)
+    runs on the host -- there is no eigensolver for non-Hermitian matrices on
+    the GPU here; the exponentials and the products of every power run
+    batched on the device.  This form is used instead of the device matrix
+    exponential, whose scaling and squaring loses accuracy on the large
+    norms of nearly singular operators (strong regularisation off, many
+    coils), while the host FP64 ``matrix_exp`` and this form agree to FP64
+    rounding."""
     dev = G_unit.device
-    L = _logm(G_unit.detach().to("cpu", torch.complex128)).to(dev)
-    e = torch.as_tensor(exponents, dtype=torch.float64, device=dev).to(L.dtype)
-    return torch.linalg.matrix_exp(e.view(-1, 1, 1) * L.unsqueeze(0))
+    L = _logm(G_unit.detach().to("cpu", torch.complex128))
+    lam, V = torch.linalg.eig(L)
+    Vi = torch.linalg.inv(V)
+    lam, V, Vi = lam.to(dev), V.to(dev), Vi.to(dev)
+    e = torch.as_tensor(exponents, dtype=torch.float64, device=dev).to(lam.dtype)
+    ph = torch.exp(e.view(-1, 1) * lam.view(1, -1))  # (n_steps, C)
+    return (V.unsqueeze(0) * ph.unsqueeze(1)) @ Vi.unsqueeze(0)
 
 
 def grappa_power(G_unit: torch.Tensor, exponents: torch.Tensor) -> torch.Tensor:

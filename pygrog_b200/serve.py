@@ -105,6 +105,8 @@ class ReconProtocol:
         """Allocate the per-slot solvers, warm cuFFT plans and the PSF for every batch
         size, and record each slot's CG loop as a CUDA graph per batch size."""
         self._cap = int(max_batch)
+        self._prepared_for = (int(max_batch), int(n_slots), bool(graphs))
+        self._solvers, self._io = {}, {}
         for s in range(n_slots):
             self._solvers[s] = BatchedDeviceCG(self.op, self._cap, self.image_shape, self.device,
                                                damp=self.damp, tol=0.0)
@@ -153,10 +155,19 @@ class ReconServer:
         self.max_batch = int(max_batch)
         self.n_slots = int(n_slots)
         self.streams = [torch.cuda.Stream(self.device) for _ in range(self.n_slots)]
+        self._key = (self.max_batch, self.n_slots, bool(graphs))
         for p in protocols.values():
             p.prepare(self.max_batch, self.n_slots, graphs=graphs)
             if p.bytes_per_request() > self.mem_budget:
                 raise ValueError(f"protocol {p.name} needs more than the memory budget for one request")
+
+    def _ensure_prepared(self) -> None:
+        """A protocol keeps the per-slot buffers and graphs of the last server
+        that prepared it; re-prepare the ones another server configuration
+        has taken over since (a protocol serves one server at a time)."""
+        for p in self.protocols.values():
+            if getattr(p, "_prepared_for", None) != self._key:
+                p.prepare(self._key[0], self._key[1], graphs=self._key[2])
 
     def _launch(self, slot: int, proto: ReconProtocol, reqs: list):
         s = self.streams[slot]
@@ -178,6 +189,8 @@ class ReconServer:
         """Serve ``requests`` (arrival times relative to the start); returns a report.
 
         ``realtime=False`` admits every request at time 0 (closed-loop throughput)."""
+        self._ensure_prepared()
+        torch.cuda.synchronize(self.device)
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         ready = {name: collections.deque() for name in self.protocols}
         free = list(range(self.n_slots))

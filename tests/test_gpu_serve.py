@@ -154,3 +154,24 @@ def test_uneven_batch_graph_matches_alone(cuda):
         if launch == 0:
             ref = _fp64_recon(protos["spiral"], data[plist.index(protos["spiral"])])
             assert rel_l2(outs[plist.index(protos["spiral"])].numpy(), ref) < 1e-4
+
+
+def test_servers_sharing_protocols_take_turns(cuda):
+    """Two servers of different batch / slot configuration over the same
+    protocols, used alternately: each re-prepares the protocols the other
+    took over, and every result equals the request reconstructed alone."""
+    protos = _protocols(cuda)
+    a = ReconServer(protos, mem_budget=2 << 30, max_batch=4, n_slots=2, device=cuda)
+    b = ReconServer(protos, mem_budget=2 << 30, max_batch=1, n_slots=1, device=cuda)
+    rng = np.random.default_rng(41)
+    done = []
+    for srv in (a, b, a):
+        reqs = _requests(protos, 8, rng)
+        rep = srv.run(reqs, realtime=False)
+        assert rep["requests"] == 8
+        done += reqs
+    for p in protos.values():
+        p.prepare(1, 1, graphs=False)
+    for r in done:
+        alone = protos[r.protocol].recon(r.data.to(cuda).unsqueeze(0), 0)[0].cpu()
+        assert rel_l2(r.result.numpy(), alone.numpy()) < 1e-5
