@@ -486,13 +486,16 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
     from pygrog_b200.serve import ReconProtocol, ReconServer, Request
     from pygrog_b200.workloads import c3_protocols
 
+    specs = c3_protocols(seed, n_slices)  # synthetic trajectories, phantoms and coil maps (not setup)
+    torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     protos = {}
-    for sp in c3_protocols(seed, n_slices):
+    for sp in specs:
         kw = dict(sp)
         name = kw.pop("name")
         protos[name] = ReconProtocol(name, kw.pop("shape"), kw.pop("coords"), kw.pop("acr"), kw.pop("smaps"),
                                      device=dev, **kw)
+    torch.cuda.synchronize(dev)
     t_proto = time.perf_counter() - t0
     gen = torch.Generator().manual_seed(seed)
     host_in = [torch.randn(p.data_shape, dtype=torch.complex64, generator=gen).pin_memory() for p in protos.values()]
@@ -530,6 +533,7 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
             "sample_coils": sc,
             "sample_coils_per_s": sc / wall, "recons_per_s": n_slices / wall, "cg_iters": 20,
             "setup_s": t_proto + t_capture, "protocols_s": t_proto, "capture_s": t_capture,
+            "protocol_ms_per_slice": t_proto * 1e3 / n_slices,
             "per_request_streams_ms": min(prev[1:]) * 1e3, "mode": "one graph, slices as branches",
             "note": "wall time incl. host<->device copies; plans, tables, PSFs and the graph built in setup"}
 
@@ -699,6 +703,13 @@ def _r(v, nd=4):
     return float(f"{v:.{nd}g}") if isinstance(v, float) else v
 
 
+def _rounded(d, nd=5):
+    """``d`` with its float values (one level deep) rounded for the one-line summary."""
+    if not isinstance(d, dict):
+        return _r(d, nd)
+    return {k: _r(v, nd) for k, v in d.items()}
+
+
 def _compact_modes(modes):
     """{mode: [fwd_ms, adj_ms, rel_err_fwd, rel_err_adj]} of the precision comparison."""
     if not isinstance(modes, dict) or "error" in modes:
@@ -720,7 +731,8 @@ def _compact_sections(coilc, cg2, c3, serving, tune):
 
     out["coil_compress_c1"] = pick(coilc, ("tc_ms", "tc_gbs", "tc_frac", "fp32_ms", "tc_rel_err_vs_fp32"))
     out["cg_sense_c2"] = pick(cg2, ("ms_per_recon", "ms_per_iter", "iter_gbs", "iter_roofline_frac"))
-    out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "setup_s", "per_request_streams_ms"))
+    out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "protocol_ms_per_slice", "capture_s",
+                                "per_request_streams_ms"))
     if isinstance(serving, dict) and "error" not in serving:
         o = serving.get("open_loop", {})
         out["serving"] = {k: _r(serving.get(k)) for k in ("closed_loop_recons_per_s", "single_instance_recons_per_s",
@@ -960,30 +972,32 @@ def main():
             "vs_baseline": None,
             "dtype": {"tc": "bf16x3 (fp32 accumulate)", "tc1": "bf16 (fp32 accumulate)"}.get(bp.mode, "fp32"),
             "data": "synthetic",
-            "accuracy": accuracy,
-            "precision_modes": _compact_modes(modes),
             "config": {
                 "workload": (f"grog3d_kooshball_{GRID_N}c{N_COILS}_{N_SPOKES}x{N_READOUT}_fwd_adj" if resized
                              else "grog3d_kooshball_192c12_fwd_adj"),
                 "grid": [GRID_N] * 3, "spokes": N_SPOKES, "readout": N_READOUT, "coils": N_COILS,
                 "kernel": "sphere w=2 (kw=4)", "precision": 1, "oversamp": 1.0,
-                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "kernels": list(bp.kernel_names()), "l2": f"inputs larger than L2 ({N * C * 8 / 1e6:.0f} MB samples, {G * C * 8 / 1e6:.0f} MB grid)",
+                "n_valid_replicas": bp.n_valid, "table_mode": bp.mode, "kernels": list(bp.kernel_names()),
+                "l2": f"inputs > L2 ({N * C * 8 / 1e6:.0f} MB samples, {G * C * 8 / 1e6:.0f} MB grid)",
                 "parallelism": f"replicas x{ws}",
             },
-            "fwd_ms": fwd_ms,
-            "adj_ms": adj_ms,
-            "setup_ms": {k: round(v, 1) for k, v in g.setup_ms.items()},
-            "roofline": {
+            "roofline": _rounded({
                 "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "algorithmic_bytes": alg_bytes,
                 "traffic": traffic, "traffic_source": tsrc,
-            },
+            }),
             "clocks": clocks,
             "gpu_launches": n_launch * args.steps,
-            "e2e": e2e,
-            "cpu_baseline": cpu,
+            "e2e": _rounded(e2e),
+            "cpu_baseline": _rounded(cpu),
+            "fwd_ms": _r(fwd_ms),
+            "adj_ms": _r(adj_ms),
+            "setup_ms": {k: round(v, 1) for k, v in g.setup_ms.items()},
             "summary": _compact_sections(coilc, cg2, c3, serving, tune),
+            # last, so that a reader keeping only the end of the output keeps them
+            "precision_modes": _compact_modes(modes),
+            "accuracy": _rounded(accuracy, 3),
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -150,12 +150,19 @@ def _default_oversamp(ndim, oversamp):
     return oversamp
 
 
-def _rescale_coords(coords: np.ndarray, amp) -> np.ndarray:
-    """``0.5 * amp * coords / max|coords|`` per axis, in float32 (``_grog.py:1318-1322``)."""
-    cmax = np.abs(coords).reshape(-1, coords.shape[-1]).max(axis=0)
+def _rescale_coords(coords: torch.Tensor, amp) -> torch.Tensor:
+    """``0.5 * amp * coords / max|coords|`` per axis, in float32 (``_grog.py:1318-1322``).
+
+    ``coords`` is a float32 ``(npts, ndim)`` tensor (on the device for plans);
+    the products and the quotient are IEEE float32 operations in the same
+    order as the reference's, so the result is bit-identical wherever it runs.
+    """
+    ndim = int(coords.shape[-1])
+    cmax = coords.abs().amax(dim=0)
     if np.isscalar(amp):
-        amp = coords.shape[-1] * [amp]
-    return 0.5 * np.asarray(amp, dtype=coords.dtype) * coords / cmax
+        amp = ndim * [amp]
+    half_amp = torch.as_tensor(0.5 * np.asarray(amp, dtype=np.float32), device=coords.device)
+    return (half_amp * coords) / cmax
 
 
 def _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, time_map, device):
@@ -164,15 +171,15 @@ def _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, tim
     Follows ``_create_plan_single`` (``_grog.py:1081-1234``); the arithmetic is
     in ``pgb_plan_geometry`` / ``pgb_plan_gauss_sum`` / ``pgb_plan_weights``.
     """
-    coords = np.asarray(coords, dtype=np.float32)
-    ndim = coords.shape[-1]
+    if not isinstance(coords, torch.Tensor):
+        coords = np.asarray(coords)
+    ndim = int(coords.shape[-1])
     if ndim not in (2, 3):
         raise ValueError(f"GROG interpolation only supports 2D or 3D data, got {ndim}D")
     shape = _default_shape(ndim, shape)
     oversamp = _default_oversamp(ndim, oversamp)
     grid_shape = tuple(int(np.ceil(s * o)) for s, o in zip(shape, oversamp))
     amp = [2 * (s - 1 - s // 2) for s in shape]
-    coords_scaled = np.ascontiguousarray(_rescale_coords(coords, amp), dtype=np.float32)
     offsets = _kernel_offsets(ndim, kernel_width, kernel_shape)
     kw = int(offsets.shape[0])
     origins = np.asarray([-(s // 2) for s in shape], dtype=np.float32)
@@ -184,7 +191,10 @@ def _create_plan_single(shape, coords, oversamp, kernel_width, kernel_shape, tim
     R = npts * kw
     G = int(np.prod(grid_shape))
     dev = torch.device(device)
-    c_d = torch.from_numpy(coords_scaled.reshape(npts, ndim)).to(dev)
+    # cast to float32 first (as the reference does), then rescale on the device
+    c_in = coords if isinstance(coords, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(coords))
+    c_d = c_in.reshape(npts, ndim).to(dev, non_blocking=False).to(torch.float32)
+    c_d = _rescale_coords(c_d, amp).contiguous()
     off_d = torch.from_numpy(np.ascontiguousarray(offsets)).to(dev)
     # per-axis parameters are read by the host launcher: pass host arrays
     gs_h = np.ascontiguousarray(grid_shape, dtype=np.int64)

@@ -15,6 +15,22 @@ def test_kernel_offsets_match_oracle(ndim, width, shape):
     np.testing.assert_array_equal(_grog._kernel_offsets(ndim, width, shape), og.kernel_offsets(ndim, width, shape))
 
 
+@pytest.mark.parametrize("ndim,dtype", [(2, np.float32), (3, np.float32), (3, np.float64)])
+def test_coordinate_rescale_is_bit_exact_with_the_oracle(ndim, dtype):
+    """The plan's coordinate rescale (a torch float32 chain, run on the GPU for
+    plans) equals the oracle's numpy float32 chain bit for bit, float64 input
+    cast to float32 first in both."""
+    rng = np.random.default_rng(ndim)
+    coords = (rng.uniform(-0.5, 0.5, (777, ndim)) * rng.uniform(0.3, 3.0)).astype(dtype)
+    shape = (96, 80, 64)[:ndim]
+    amp = [2 * (s - 1 - s // 2) for s in shape]
+    c32 = np.asarray(coords, dtype=np.float32)
+    want = 0.5 * np.asarray(amp, dtype=np.float32) * c32 / np.abs(c32).reshape(-1, ndim).max(axis=0)
+    got = _grog._rescale_coords(torch.from_numpy(coords).to(torch.float32), amp).numpy()
+    assert got.dtype == np.float32
+    np.testing.assert_array_equal(got, want)
+
+
 @pytest.mark.parametrize("case", golden_plan_cases())
 def test_table_fit_matches_reference(case):
     """Host LAPACK table fit == the reference's table (same library calls)."""
