@@ -106,12 +106,17 @@ __global__ void __launch_bounds__(256) coil_compress_kernel(const float2* __rest
 }
 
 // ---- tensor-core compression ---------------------------------------------------
-// out = mat @ data as D (2 KP x 8 samples) = A (2 KP x 2 CIP) B (2 CIP x 8): A is
-// the realified matrix with rows [Re out 0..7 | Im out 0..7] per 16-row tile, so
-// a lane's two accumulator rows g and g + 8 are the real and imaginary parts of
-// output coil g; B is 8 samples with (re, im) of every input coil interleaved
-// along k, loaded straight from the coil planes (8 samples x 4 coils per load).
-// bf16x3: A = Ah + Al, B = Bh + Bl, D = Al Bh + Ah Bl + Ah Bh in FP32.
+// out = mat @ data, one 16-sample m-tile per warp and stage:
+// D (16 samples x 8 NT) = A (16 samples x 2 CIP) B (2 CIP x 8 NT).  A holds the
+// samples with (re, im) of every input coil interleaved along k, so each A word
+// of a lane is one staged float2 sample (input coil 8 kc + t (+ 4), samples g
+// and g + 8); B is the realified matrix with (re, im) of every output coil
+// interleaved along n, held in registers, so the accumulator pairs (c0, c1) and
+// (c2, c3) of a lane are the complex outputs of output coil 4 nt + t at samples
+// g and g + 8.  12 output coils fill three n-tiles exactly.
+// bf16x3: A = Ah + Al, B = Bh + Bl, D = Al Bh + Ah Bl + Ah Bh in FP32, with two
+// accumulators per n-tile (even and odd k steps) so that the dependent MMA
+// chains are half as long.
 __device__ __forceinline__ void mma16c(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};\n"
@@ -132,9 +137,9 @@ __device__ __forceinline__ void split_bf2(float x, float y, uint32_t& hi, uint32
 // Samples move in chunks of kCS per CTA stage (all input coils), staged in
 // shared memory by 16-byte async copies kStages deep (in-flight bytes are what
 // bound this HBM pass), coil stride kCS + 4 float2 so the four coils a lane
-// quad reads fall in different banks.  Each warp computes two 8-sample tiles
+// quad reads fall in different banks.  Each warp computes one 16-sample m-tile
 // per stage.
-constexpr int kCS = 128;     // samples per chunk (8 warps x two 8-sample tiles)
+constexpr int kCS = 128;     // samples per chunk (8 warps x one 16-sample m-tile)
 constexpr int kStages = 3;   // chunks in flight per CTA
 constexpr int kXS = kCS + 4; // shared-memory coil stride (float2)
 
@@ -147,37 +152,36 @@ __device__ __forceinline__ void cpa8(void* dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 
-template <int CIP, int KT>  // CIP input coils (multiple of 8), KT 16-row tiles (8 output coils each)
+template <int CIP, int NT>  // CIP input coils (multiple of 8), NT n-tiles (4 output coils each)
 __global__ void __launch_bounds__(256, 2) coil_compress_tc_kernel(const float2* __restrict__ data, int64_t N, int C,
                                                                   int K, int B, const float2* __restrict__ mat,
                                                                   float2* __restrict__ out) {
-  constexpr int KC = CIP / 8;  // k16 chunks (8 input coils each)
+  constexpr int KC = CIP / 8;  // k16 steps (8 input coils each)
   extern __shared__ __align__(16) float2 xs_flat[];  // kStages buffers of CIP x kXS
   auto xs = [&](int k) { return xs_flat + k * (CIP * kXS); };
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
-  // A fragments of the realified matrix, heads and tails:
-  // A[r][2c] = Re / Im part, A[r][2c + 1] = -Im / Re part (row r < 8: Re of out coil r, else Im)
-  uint32_t ah[KT][KC][4], al[KT][KC][4];
+  // B fragments of the realified matrix, heads and tails: b0 covers k rows 2t,
+  // 2t + 1 (re, im of input coil 8 kc + t), b1 input coil 8 kc + t + 4; column
+  // g is the real (even g) or imaginary (odd g) part of output coil 4 nt + g / 2
+  uint32_t bh[NT][KC][2], bl[NT][KC][2];
 #pragma unroll
-  for (int T = 0; T < KT; ++T)
+  for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
     for (int kc = 0; kc < KC; ++kc)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int row = g + ((q & 1) ? 8 : 0);       // a0/a2: row g, a1/a3: row g + 8
-        const int c = 8 * kc + t + ((q & 2) ? 4 : 0);  // a0/a1: k cols 2t.., a2/a3: 2t + 8..
-        const int ko = 8 * T + (row & 7);
+      for (int h = 0; h < 2; ++h) {
+        const int ko = 4 * nt + (g >> 1);
+        const int c = 8 * kc + t + 4 * h;
         float2 m = make_float2(0.f, 0.f);
         if (ko < K && c < C) m = __ldg(mat + ko * C + c);
-        const float e0 = row < 8 ? m.x : m.y;   // times x_re
-        const float e1 = row < 8 ? -m.y : m.x;  // times x_im
-        split_bf2(e0, e1, ah[T][kc][q], al[T][kc][q]);
+        const float e0 = (g & 1) ? m.y : m.x;   // times x_re
+        const float e1 = (g & 1) ? m.x : -m.y;  // times x_im
+        split_bf2(e0, e1, bh[nt][kc][h], bl[nt][kc][h]);
       }
   const int64_t chunks_per_b = (N + kCS - 1) / kCS;
   const int64_t n_chunks = static_cast<int64_t>(B) * chunks_per_b;
   // 16-byte copies need even N and a 16-byte aligned base (pairs of samples)
   const bool wide = (N & 1) == 0 && (reinterpret_cast<uintptr_t>(data) & 15) == 0;
-  const bool wide_out = (N & 1) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
   // stage chunk q (all coils) into buffer k; q >= n_chunks commits an empty group
   auto stage = [&](int64_t q, int k) {
     if (q < n_chunks) {
@@ -212,42 +216,43 @@ __global__ void __launch_bounds__(256, 2) coil_compress_tc_kernel(const float2* 
     __syncthreads();
     stage(q + (kStages - 1) * stride, (it + kStages - 1) % kStages);
     const int64_t b = q / chunks_per_b;
-#pragma unroll 1
-    for (int tile = warp; tile < kCS / 8; tile += 8) {
-    const int64_t n0 = (q - b * chunks_per_b) * kCS + 8 * tile;  // this warp's 8-sample tile
+    const int64_t n0 = (q - b * chunks_per_b) * kCS + 16 * warp;  // this warp's 16-sample m-tile
     if (n0 < N) {
-      const float2* x = xs(k) + 8 * tile + g;  // sample g of the tile
-      uint32_t bh[KC][2], bl[KC][2];
+      const float2* x = xs(k) + 16 * warp + g;  // sample g of the m-tile
+      float d[NT][2][4];
 #pragma unroll
-      for (int kc = 0; kc < KC; ++kc)
+      for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float2 v = x[(8 * kc + t + 4 * h) * kXS];  // coil 8 kc + t + 4 h (zero beyond C)
-          split_bf2(v.x, v.y, bh[kc][h], bl[kc][h]);
+        for (int j = 0; j < 2; ++j) d[nt][j][0] = d[nt][j][1] = d[nt][j][2] = d[nt][j][3] = 0.f;
+#pragma unroll
+      for (int kc = 0; kc < KC; ++kc) {
+        // a0 / a1: input coil 8 kc + t at samples g / g + 8; a2 / a3: coil 8 kc + t + 4
+        // (staged planes are zero beyond C and beyond N)
+        uint32_t ah[4], al[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const float2 v = x[(8 * kc + t + 4 * (r >> 1)) * kXS + 8 * (r & 1)];
+          split_bf2(v.x, v.y, ah[r], al[r]);
         }
 #pragma unroll
-      for (int T = 0; T < KT; ++T) {
-        float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kc = 0; kc < KC; ++kc) {
-          mma16c(d, al[T][kc], bh[kc][0], bh[kc][1]);
-          mma16c(d, ah[T][kc], bl[kc][0], bl[kc][1]);
-          mma16c(d, ah[T][kc], bh[kc][0], bh[kc][1]);
-        }
-        // d[0], d[1]: Re of out coil 8T + g at samples 2t, 2t + 1; d[2], d[3]: Im
-        const int ko = 8 * T + g;
-        const int64_t n = n0 + 2 * t;
-        if (ko < K && n < N) {
-          float2* dst = out + (b * K + ko) * N + n;
-          if (wide_out && n + 1 < N) {
-            *reinterpret_cast<float4*>(dst) = make_float4(d[0], d[2], d[1], d[3]);
-          } else {
-            dst[0] = make_float2(d[0], d[2]);
-            if (n + 1 < N) dst[1] = make_float2(d[1], d[3]);
-          }
+        for (int nt = 0; nt < NT; ++nt) {
+          float(&acc)[4] = d[nt][kc & 1];
+          mma16c(acc, al, bh[nt][kc][0], bh[nt][kc][1]);
+          mma16c(acc, ah, bl[nt][kc][0], bl[nt][kc][1]);
+          mma16c(acc, ah, bh[nt][kc][0], bh[nt][kc][1]);
         }
       }
-    }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int ko = 4 * nt + t;
+        if (ko < K) {
+          float2* dst = out + (b * K + ko) * N + n0 + g;
+          const float* e = d[nt][0];
+          const float* o = d[nt][1];
+          if (n0 + g < N) dst[0] = make_float2(e[0] + o[0], e[1] + o[1]);
+          if (n0 + g + 8 < N) dst[8] = make_float2(e[2] + o[2], e[3] + o[3]);
+        }
+      }
     }
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -324,19 +329,20 @@ int pgb_coil_compress_tc(const void* data, int64_t N, int64_t C, int64_t K, int6
   const int64_t chunks = B * ((N + kCS - 1) / kCS);
   const int blocks = static_cast<int>(chunks < 148 * 2 ? chunks : 148 * 2);  // persistent: two CTAs per SM
   const int cip = static_cast<int>((C + 7) / 8 * 8);
-  const int kt = K > 8 ? 2 : 1;
+  const int nt = static_cast<int>((K + 3) / 4);
   const float2* d = static_cast<const float2*>(data);
   const float2* m = static_cast<const float2*>(mat);
   float2* o = static_cast<float2*>(out);
   const int Ci = static_cast<int>(C), Ki = static_cast<int>(K), Bi = static_cast<int>(B);
-  switch (cip * 10 + kt) {
-#define X(CI, KTT)                                                                                  \
-  case CI * 10 + KTT: {                                                                             \
+  switch (cip * 10 + nt) {
+#define X(CI, NTT)                                                                                  \
+  case CI * 10 + NTT: {                                                                             \
     const int smem = kStages * CI * kXS * static_cast<int>(sizeof(float2));                         \
-    cudaFuncSetAttribute(coil_compress_tc_kernel<CI, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
-    coil_compress_tc_kernel<CI, KTT><<<blocks, 256, smem, s>>>(d, N, Ci, Ki, Bi, m, o);              \
+    cudaFuncSetAttribute(coil_compress_tc_kernel<CI, NTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
+    coil_compress_tc_kernel<CI, NTT><<<blocks, 256, smem, s>>>(d, N, Ci, Ki, Bi, m, o);              \
   } break;
-    X(8, 1) X(16, 1) X(16, 2) X(24, 1) X(24, 2) X(32, 1) X(32, 2)
+    X(8, 1) X(8, 2) X(16, 1) X(16, 2) X(16, 3) X(16, 4) X(24, 1) X(24, 2) X(24, 3) X(24, 4)
+    X(32, 1) X(32, 2) X(32, 3) X(32, 4)
 #undef X
     default:
       PGB_REQUIRE(false, PGB_ERR_UNSUPPORTED, "%s: no kernel for C=%lld K=%lld", who, (long long)C, (long long)K);
