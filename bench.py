@@ -698,6 +698,64 @@ def time_calls(dev, reps: int = 5) -> dict:
     return out
 
 
+def chain_compare(dev, n_rep: int = 7_680_208, coils=(12, 32), reps: int = 5, seed: int = 1007) -> dict:
+    """The eigen-factored shift chain alone (``pgb_shift_chain``) with mma.sync and
+    with tcgen05 (accumulator in tensor memory), on ``n_rep`` replicas (the c1
+    valid-replica count) at 12 and 32 coils: CUDA-event time of one launch
+    applying the chain once and four times (best of ``reps``), the chain's own
+    time per application ((t4 - t1) / 3, loads and stores excluded), and the
+    relative error of the single chain against an FP64 restatement on every
+    997th replica.  Random unitary W and unit-modulus phases keep repeated
+    chains bounded."""
+    import torch
+
+    from pygrog_b200.calib import _chain
+
+    rng = np.random.default_rng(seed)
+    res = {"replicas": n_rep}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for C in coils:
+        W = np.stack([np.linalg.qr(rng.standard_normal((C, C)) + 1j * rng.standard_normal((C, C)))[0]
+                      for _ in range(4)])
+        ph = np.exp(1j * rng.uniform(-np.pi, np.pi, (3, _chain.STEPS, C)))
+        Wd, phd = _chain.chain_operands(W, ph, dev)
+        gen = torch.Generator(device=dev).manual_seed(seed + C)
+        x = torch.randn(2 * C, n_rep, device=dev, generator=gen)
+        ijk = torch.randint(0, _chain.STEPS, (3, n_rep), device=dev, generator=gen)
+        idx = _chain.pack_shift_indices(ijk)
+        out = torch.empty_like(x)
+        rows = np.arange(0, n_rep, 997)
+        xs = x[:, rows].double().cpu().numpy()
+        y = xs[0::2] + 1j * xs[1::2]
+        ii = ijk[:, rows].cpu().numpy()
+        for s in range(4):
+            y = W[s] @ y
+            if s < 3:
+                y = y * ph[s][ii[s]].T
+        for variant in ("mma", "tcgen05"):
+            key = f"c{C}_{variant}"
+            t = torch.zeros(1, dtype=torch.int32, device=dev)
+            for rep in (1, 4):
+                ts = []
+                for it in range(reps + 2):
+                    ev[0].record()
+                    _chain.shift_chain(x, idx, Wd, phd, out, rep=rep, variant=variant, timeouts=t)
+                    ev[1].record()
+                    torch.cuda.synchronize(dev)
+                    if it >= 2:
+                        ts.append(ev[0].elapsed_time(ev[1]))
+                res[f"{key}_rep{rep}_ms"] = min(ts)
+                if rep == 1:
+                    o = out[:, rows].double().cpu().numpy()
+                    res[f"{key}_rel_err_vs_fp64"] = float(np.linalg.norm(o[0::2] + 1j * o[1::2] - y) / np.linalg.norm(y))
+            _chain.check_timeouts(t)
+            res[f"{key}_chain_ms"] = (res[f"{key}_rep4_ms"] - res[f"{key}_rep1_ms"]) / 3
+        res[f"c{C}_tcgen05_speedup"] = res[f"c{C}_mma_chain_ms"] / res[f"c{C}_tcgen05_chain_ms"]
+        del x, out, idx, ijk
+        torch.cuda.empty_cache()
+    return res
+
+
 def _r(v, nd=4):
     """Round floats for the one-line summary (None and non-floats pass)."""
     return float(f"{v:.{nd}g}") if isinstance(v, float) else v
@@ -770,6 +828,10 @@ def main():
                     help="only time the public API call by call on configs c0 and c2 (one JSON line)")
     ap.add_argument("--coil-only", action="store_true",
                     help="only time the coil compression (32 -> --coils) of --spokes x --readout samples (one JSON line)")
+    ap.add_argument("--chain", action="store_true",
+                    help="only time the shift chain alone, mma.sync against tcgen05, at 12 and 32 coils (one JSON line)")
+    ap.add_argument("--chain-replicas", type=int, default=7_680_208, help="replicas of --chain (default: c1's valid replicas)")
+    ap.add_argument("--chain-coils", default="12,32", help="coil counts of --chain (12 and / or 32)")
     ap.add_argument("--serve-sweep", action="store_true",
                     help="only sweep open-loop arrival rates of the served mix, batched vs single-instance (one JSON line)")
     ap.add_argument("--details", default=None,
@@ -802,6 +864,13 @@ def main():
             r = coil_compress_c1(dev)
             print(json.dumps({"coil_compress": {k: v for k, v in r.items() if not isinstance(v, dict)},
                               "samples": N_SPOKES * N_READOUT}), flush=True)
+        return 0
+    if args.chain:
+        if rank == 0:
+            coils = tuple(int(c) for c in args.chain_coils.split(","))
+            r = chain_compare(dev, n_rep=args.chain_replicas, coils=coils)
+            print(json.dumps({"shift_chain": {k: _r(v) for k, v in r.items()},
+                              "device": torch.cuda.get_device_name(dev)}), flush=True)
         return 0
     if args.serve_sweep:
         if rank == 0:

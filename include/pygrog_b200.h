@@ -346,6 +346,22 @@ PGB_API int pgb_grog_tc_timeouts(int64_t* count, int64_t reset);
  * No reference counterpart (failure-path testing). */
 PGB_API int pgb_grog_tc_wait_limit(int64_t limit, int64_t* previous);
 
+/* The eigen-factored shift chain alone, y = W3 Dx[k] W2 Dy[j] W1 Dz[i] W0 x on
+ * R replicas (the table product of calib/_grappa.py:62-72, 184-208 applied to
+ * one replica, as the tensor-core gridders run it), in two tensor-core forms,
+ * for measuring the MMA flavour: variant 0 = mma.sync with the accumulators
+ * handed on in registers, variant 1 = tcgen05.mma with the accumulator in
+ * tensor memory (M = 128 replicas per tile).  bf16x3 products, FP32
+ * accumulation.  C = 12 or 32 coils.  x, out: (2C, R) float realified
+ * (row 2c real part of coil c, 2c + 1 imaginary); idx: R int32
+ * i | j << 8 | k << 16, each < 11; W: (4, 2C, 2C) float realified
+ * [stage][output][input]; ph: (3, 11, C) complex64 phases.  rep >= 1 applies
+ * the chain rep times per loaded tile.  timeouts: int32 device counter
+ * (required for variant 1), incremented by every CTA whose bounded tensor-core
+ * waits ran out.  Asynchronous on `stream`.  No reference counterpart. */
+PGB_API int pgb_shift_chain(const void* x, const void* idx, const void* W, const void* ph, void* out, int64_t R,
+                            int64_t C, int64_t rep, int64_t variant, void* timeouts, void* stream);
+
 /* =====================================================================
  * Coil compression (the step before the path)
  * ===================================================================== */

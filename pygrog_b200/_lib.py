@@ -120,6 +120,7 @@ _SIGS = {
     "pgb_grog_tc_use_tma": [_i64],
     "pgb_grog_tc_timeouts": [_vp, _i64],
     "pgb_grog_tc_wait_limit": [_i64, _vp],
+    "pgb_shift_chain": [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp],
     "pgb_lsmr_u_update": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_lsmr_u_scale": [_vp, _i64, _vp, _vp],
     "pgb_lsmr_v_full": [_vp, _vp, _vp, _i64, _vp, _vp, _vp],

@@ -20,7 +20,7 @@ PKG = CSRC.parent
 REPO = PKG.parent
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libpygrog_b200.so"
-SOURCES = ["l0_ops.cu", "plan.cu", "grog_fused.cu", "grog_v6.cu", "grog_v8.cu", "grog_tc.cu", "coil.cu", "fft_stage.cu", "solver.cu", "lsmr.cu", "subspace.cu", "plan_pack.cu"]
+SOURCES = ["l0_ops.cu", "plan.cu", "grog_fused.cu", "grog_v6.cu", "grog_v8.cu", "grog_tc.cu", "coil.cu", "fft_stage.cu", "solver.cu", "lsmr.cu", "subspace.cu", "plan_pack.cu", "shift_chain.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
