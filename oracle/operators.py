@@ -222,3 +222,51 @@ def sub_toeplitz_normal(x, P, grid_shape, image_shape, smaps):
         mixed = np.einsum("...ab,b...->a...", P, Kk)
         out += np.conj(smaps[c]) * ifftc(mixed, axes)[sl]
     return out
+
+
+# ---- SubspaceMaskedFFT (gadgets/_subspace.py:761-1004, _toep/_sub_toep.py:64-117) ----
+def submasked_tcell(grid_shape, t_axis):
+    """Encoding (frame) index of every grid cell: its coordinate along ``t_axis``."""
+    T = grid_shape[t_axis]
+    shp = [1] * len(grid_shape)
+    shp[t_axis] = T
+    return np.broadcast_to(np.arange(T).reshape(shp), grid_shape).reshape(-1)
+
+
+def submasked_adjoint(kgrid, mask, basis, t_axis, grid_shape, image_shape, smaps):
+    """kgrid (C, *grid) -> (K, *img): x_k = sum_c conj(S_c) crop(ifftc(mask * basis[k, t] * y_c)),
+    the centred transform over every grid axis (``_subspace.py:879-907``)."""
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    K = basis.shape[0]
+    phi = basis[:, submasked_tcell(grid_shape, t_axis)].reshape(K, *grid_shape)
+    sl = (slice(None), *_slices(grid_shape, image_shape))
+    out = np.zeros((K, *image_shape), dtype=np.complex128)
+    for c in range(kgrid.shape[0]):
+        out += np.conj(smaps[c]) * ifftc(phi * kgrid[c] * mask, axes)[sl]
+    return out
+
+
+def submasked_forward(x, mask, basis, t_axis, grid_shape, image_shape, smaps):
+    """(K, *img) -> (C, *grid): y_c = sum_k conj(basis[k, t]) mask fftc(pad(S_c x_k)) (``_subspace.py:950-988``)."""
+    nd = len(grid_shape)
+    axes = tuple(range(-nd, 0))
+    K = basis.shape[0]
+    phi = basis[:, submasked_tcell(grid_shape, t_axis)].reshape(K, *grid_shape)
+    sl = (slice(None), *_slices(grid_shape, image_shape))
+    out = np.zeros((smaps.shape[0], *grid_shape), dtype=np.complex128)
+    for c in range(smaps.shape[0]):
+        pad = np.zeros((K, *grid_shape), dtype=np.complex128)
+        pad[sl] = smaps[c] * x
+        out[c] = (np.conj(phi) * fftc(pad, axes) * mask).sum(0)
+    return out
+
+
+def submasked_psf(density, basis, t_axis, grid_shape):
+    """The reference's masked PSF (``_sub_toep.py:64-105``): P[j, a, b] = density[j] *
+    basis[b, t_j] * conj(basis[a, t_j]) -> (*grid, K, K); applied by
+    :func:`sub_toeplitz_normal` as out_a = sum_b P[a, b] in_b."""
+    K = basis.shape[0]
+    Bj = basis[:, submasked_tcell(grid_shape, t_axis)].T  # (G, K)
+    P = density.reshape(-1, 1, 1) * (np.conj(Bj)[:, :, None] * Bj[:, None, :])
+    return P.reshape(*grid_shape, K, K)

@@ -3,6 +3,7 @@
 from ._masked_fft import MaskedFFT, MaskedFFTPlan  # noqa: F401
 from ._sparse_fft import SparseFFT, gather, scatter_add  # noqa: F401
 from ._subspace import (  # noqa: F401
+    SubspaceMaskedFFT,
     SubspaceProjection,
     SubspaceSparseFFT,
     SubspaceToeplitzOp,
@@ -10,4 +11,4 @@ from ._subspace import (  # noqa: F401
 )
 
 __all__ = ["SparseFFT", "MaskedFFT", "MaskedFFTPlan", "gather", "scatter_add", "SubspaceProjection",
-           "SubspaceSparseFFT", "SubspaceToeplitzOp", "with_subspace"]
+           "SubspaceMaskedFFT", "SubspaceSparseFFT", "SubspaceToeplitzOp", "with_subspace"]

@@ -14,11 +14,23 @@ FiRMLAB-Pisa/pygrog.  With basis ``Phi (K, T)`` and the sample weights
 The reference loops over coils and components with one scatter / FFT per
 (c, k); here one kernel reads every sample once for all K components, the
 FFTs run batched over (frames, K, C), and the K x K PSF matvec is one kernel.
+
+``SubspaceMaskedFFT`` (``gadgets/_subspace.py:761-1004``) wraps a
+:class:`MaskedFFT` whose grid carries the encoding axis: with ``t(g)`` the
+encoding index of grid cell ``g`` and the reference's centred transform over
+every grid axis,
+
+    forward:  y_c = sum_k conj(Phi[k, t]) * mask * FFT(pad(S_c x_k))
+    adjoint:  x_k = sum_c conj(S_c) crop(IFFT(mask * Phi[k, t] * y_c))
+    normal (Toeplitz): the K x K PSF P[g, a, b] = density[g] Phi[b, t(g)]
+              conj(Phi[a, t(g)]) of ``_toep/_sub_toep.py:64-105`` (the
+              reference builds the masked PSF in this order; for a complex
+              basis it is the conjugate of the nested operator's).
 """
 
 from __future__ import annotations
 
-__all__ = ["SubspaceProjection", "SubspaceSparseFFT", "SubspaceToeplitzOp", "with_subspace"]
+__all__ = ["SubspaceMaskedFFT", "SubspaceProjection", "SubspaceSparseFFT", "SubspaceToeplitzOp", "with_subspace"]
 
 import numpy as np
 import torch
@@ -58,11 +70,12 @@ class SubspaceProjection:
 
 
 def with_subspace(base_op, subspace_basis, encoding_axis: int = -4, *, toeplitz=None):
-    """Wrap a :class:`SparseFFT` with a subspace projection (reference ``with_subspace``)."""
+    """Wrap a :class:`SparseFFT` or :class:`MaskedFFT` with a subspace projection
+    (reference ``with_subspace``, ``gadgets/_subspace.py:91-122``)."""
     from ._masked_fft import MaskedFFT
 
     if isinstance(base_op, MaskedFFT):
-        raise NotImplementedError("the subspace decorator covers SparseFFT operators")
+        return SubspaceMaskedFFT(base_op, subspace_basis, encoding_axis=encoding_axis, toeplitz=toeplitz)
     return SubspaceSparseFFT(base_op, subspace_basis, encoding_axis=encoding_axis, toeplitz=toeplitz)
 
 
@@ -238,10 +251,96 @@ class SubspaceSparseFFT(SolveMixin):
         return out
 
 
+class SubspaceMaskedFFT(SubspaceSparseFFT):
+    """MaskedFFT with low-rank subspace projection (reference ``SubspaceMaskedFFT``,
+    ``gadgets/_subspace.py:761-1004``).
+
+    The base operator's grid (its natural shape) carries the encoding axis
+    ``T`` (``encoding_axis`` counts in the layout ``(C, *grid)``; default -3:
+    ``(C, T, gy, gx)``).  Gridded k-space ``(*B, *S, C, *grid)`` <->
+    coefficients ``(*B, *S, K, *image)``; as in the reference, the centred
+    transforms run over every grid axis and the crop pairs grid and image
+    axes in order, so the image shape has the grid's rank.  All coils and
+    components go through one batched masked transform per stack element.
+    """
+
+    def __init__(self, base_op, subspace_basis, encoding_axis: int = -3, *, toeplitz=None):
+        self._base = base_op
+        self.basis = torch.as_tensor(subspace_basis)
+        self.K, self.T = (int(v) for v in self.basis.shape)
+        self.encoding_axis = encoding_axis
+        self.k_chunk = 1
+        self.grid_shape = tuple(base_op.grid_shape)
+        self.image_shape = tuple(base_op.image_shape)
+        self.natural_shape = tuple(base_op.natural_shape)  # the grid
+        self.stack_shape = tuple(getattr(base_op, "stack_shape", ()) or ())
+        self.smaps = getattr(base_op, "smaps", None)
+        nat_ndim = len(self.natural_shape)
+        ax = encoding_axis if encoding_axis >= 0 else encoding_axis + (1 + nat_ndim)
+        self._t_axis_in_nat = ax - 1
+        if not (0 <= self._t_axis_in_nat < nat_ndim):
+            raise ValueError(
+                f"encoding_axis={encoding_axis} does not land inside natural_shape "
+                f"{base_op.natural_shape} (computed nat-axis {self._t_axis_in_nat})"
+            )
+        if self.natural_shape[self._t_axis_in_nat] != self.T:
+            raise ValueError(
+                f"basis T={self.T} does not match natural_shape"
+                f"[{self._t_axis_in_nat}]={self.natural_shape[self._t_axis_in_nat]}"
+            )
+        if toeplitz is None:
+            toeplitz = bool(getattr(base_op, "toeplitz", False))
+        if toeplitz and getattr(base_op, "density", None) is None:
+            raise ValueError("a Toeplitz SubspaceMaskedFFT needs base_op.density")
+        self.toeplitz = bool(toeplitz)
+        self._toep_op = None
+        self._cdev = base_op._cdev
+        self._single_ndim = 1 + len(self.image_shape)
+        dev = self._cdev
+        self._basis_d = as_c64(self.basis, dev).contiguous()
+        view = [1] * nat_ndim
+        view[self._t_axis_in_nat] = self.T
+        # encoding index of every grid cell, and Phi[k, t(g)] on the grid
+        self._tcell = (torch.arange(self.T, dtype=torch.int64, device=dev).view(view)
+                       .expand(self.natural_shape).reshape(-1).contiguous())
+        G = int(np.prod(self.grid_shape))
+        self._phi = self._basis_d[:, self._tcell].reshape(1, self.K, 1, G).contiguous()
+        self._phi_conj = self._phi.conj().contiguous()
+
+    def _require_smaps(self):
+        if self._base.smaps is None:
+            raise NotImplementedError("SubspaceMaskedFFT requires base_op.smaps")
+
+    def _adjoint_core(self, y: torch.Tensor, s: int) -> torch.Tensor:
+        """y (Bt, C, G) centred grid -> (Bt, K, *image): mask, Phi[k, t], IFFT, crop, coil sum."""
+        Bt, C, G = (int(v) for v in y.shape)
+        st = self._base._stage
+        w = (y.reshape(Bt, 1, C, G) * self._phi).contiguous()  # (Bt, K, C, G)
+        u = torch.empty(Bt, self.K, C, *st.grid_shape, dtype=torch.complex64, device=y.device)
+        st.shift(w, self._base._mask_d[s], u, Bt * self.K * C, 1.0, to_centred=False)
+        v = st.ifft(u)
+        out = torch.empty(Bt, self.K, *st.image_shape, dtype=torch.complex64, device=y.device)
+        st.combine(v, self._base._smaps_d, out, Bt * self.K, C, st.ortho)
+        return out
+
+    def _forward_core(self, x: torch.Tensor, s: int) -> torch.Tensor:
+        """x (Bt, K, *image) -> (Bt, C, G) centred grid: smaps, pad, FFT, mask, sum_k conj(Phi[k, t])."""
+        Bt = int(x.shape[0])
+        st = self._base._stage
+        sm = self._base._smaps_d
+        C = int(sm.shape[0])
+        u = torch.empty(Bt, self.K, C, *st.grid_shape, dtype=torch.complex64, device=x.device)
+        st.expand(x, sm, u, Bt * self.K, C, 1.0, x_has_coils=False)
+        U = st.fft(u)
+        o = torch.empty_like(U)
+        st.shift(U, self._base._mask_d[s], o, Bt * self.K * C, st.ortho, to_centred=True)
+        return (o.reshape(Bt, self.K, C, st.G) * self._phi_conj).sum(1)
+
+
 class SubspaceToeplitzOp:
-    """``A^H A`` of a :class:`SubspaceSparseFFT` with a per-cell K x K PSF
-    (reference ``SubspaceToeplitzOp``; ``psf`` holds the PSF on the centred
-    grid in the reference's ``(*grid, K, K)`` layout)."""
+    """``A^H A`` of a :class:`SubspaceSparseFFT` or :class:`SubspaceMaskedFFT`
+    with a per-cell K x K PSF (reference ``SubspaceToeplitzOp``; ``psf`` holds
+    the PSF on the centred grid in the reference's ``(*grid, K, K)`` layout)."""
 
     def __init__(self, sub_op: SubspaceSparseFFT, device=None):
         base = sub_op._base
@@ -256,22 +355,30 @@ class SubspaceToeplitzOp:
         self.stack_shape = sub_op.stack_shape
         st = base._stage
         S = int(np.prod(self.stack_shape)) if self.stack_shape else 1
-        nat = sub_op.natural_shape
-        n_per = int(np.prod(nat))
-        t_nat = sub_op._tidx.to(torch.int64)
-        idx_all = base.indices.reshape(S, -1).to(self.device)
-        sw_all = base.sqrt_weights.reshape(S, -1).to(self.device, torch.float32)
-        sp_all = base.sort_perm.reshape(S, -1).to(self.device)
         basis = sub_op._basis_d
-        psfs = []
-        for s in range(S):
-            w = sw_all[s] * sw_all[s]
-            w_eff = (w * w).contiguous()
-            t_sorted = t_nat[sp_all[s] % n_per].contiguous()
-            pf = torch.zeros(st.G, self.K, self.K, dtype=torch.complex64, device=self.device)
-            _ext.psf_scatter_outer_basis(pf, idx_all[s].contiguous(), w_eff, basis, t_sorted)
-            psfs.append(pf.transpose(-2, -1).contiguous())  # P[g, k, k']
-        P = torch.stack(psfs).reshape(S, *self.grid_shape, self.K, self.K)
+        if isinstance(sub_op, SubspaceMaskedFFT):
+            # one encoding index per grid cell: P[g, a, b] = density[g] Phi[b, t(g)]
+            # conj(Phi[a, t(g)]), in the order of _toep/_sub_toep.py:64-105
+            dens = base.density.to(self.device, torch.float32).reshape(S, st.G)
+            Bj = basis[:, sub_op._tcell].T  # (G, K): Phi[k, t(g)]
+            P = dens.reshape(S, st.G, 1, 1) * (Bj.conj()[None, :, :, None] * Bj[None, :, None, :])
+            P = P.to(torch.complex64).reshape(S, *self.grid_shape, self.K, self.K)
+        else:
+            nat = sub_op.natural_shape
+            n_per = int(np.prod(nat))
+            t_nat = sub_op._tidx.to(torch.int64)
+            idx_all = base.indices.reshape(S, -1).to(self.device)
+            sw_all = base.sqrt_weights.reshape(S, -1).to(self.device, torch.float32)
+            sp_all = base.sort_perm.reshape(S, -1).to(self.device)
+            psfs = []
+            for s in range(S):
+                w = sw_all[s] * sw_all[s]
+                w_eff = (w * w).contiguous()
+                t_sorted = t_nat[sp_all[s] % n_per].contiguous()
+                pf = torch.zeros(st.G, self.K, self.K, dtype=torch.complex64, device=self.device)
+                _ext.psf_scatter_outer_basis(pf, idx_all[s].contiguous(), w_eff, basis, t_sorted)
+                psfs.append(pf.transpose(-2, -1).contiguous())  # P[g, k, k']
+            P = torch.stack(psfs).reshape(S, *self.grid_shape, self.K, self.K)
         self.psf = P[0] if not self.stack_shape else P.reshape(*self.stack_shape, *self.grid_shape, self.K, self.K)
         # FFT order, 1/G of the two unscaled transforms folded in
         Pf = torch.fft.ifftshift(P, dim=tuple(range(1, 1 + len(self.grid_shape))))

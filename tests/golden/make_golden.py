@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (see ``refimport.py``):
 
-    python tests/golden/make_golden.py [plans] [l0] [operators] [subspace]
+    python tests/golden/make_golden.py [plans] [l0] [operators] [subspace] [submasked]
 
 Writes ``tests/golden/*.npz``.  Every array stored under ``ref_*`` is an output
 of the reference implementation itself (its Python package plus its C++
@@ -234,6 +234,44 @@ def make_subspace_cases(pg, out):
     print("wrote sub2d")
 
 
+def make_subspace_masked_case(pg, out):
+    """SubspaceMaskedFFT adjoint / forward / normal (Toeplitz with the density
+    PSF, and nested) / CG on a MaskedFFT whose grid (T, gy, gx) carries T = 5
+    frames on its first axis (encoding axis -3 of the layout (C, T, gy, gx));
+    the reference transforms and crops every grid axis, so the image shape
+    has the grid's rank (T, ny, nx)."""
+    import importlib
+
+    gad = importlib.import_module("pygrog.gadgets")
+    rng = np.random.default_rng(2025)
+    grid, img, C, K, T = (5, 12, 10), (5, 8, 8), 3, 2, 5
+    mask = (rng.random(grid) < 0.55).astype(np.float32)
+    density = (mask * rng.uniform(0.5, 2.0, grid)).astype(np.float32)
+    smaps = (_c(rng, C, *img) * 0.5).astype(np.complex64)
+    q, _ = np.linalg.qr(_c(rng, T, K, dtype=np.complex128))
+    basis = q.T.astype(np.complex64)  # (K, T) orthonormal rows
+    mk = dict(grid_shape=grid, image_shape=img, mask=torch.from_numpy(mask), density=torch.from_numpy(density),
+              smaps=torch.from_numpy(smaps))
+    base_t = pg.operator.MaskedFFT(**mk, toeplitz=True)
+    base_n = pg.operator.MaskedFFT(**mk, toeplitz=False)
+    sub_t = gad.with_subspace(base_t, torch.from_numpy(basis), encoding_axis=-3)
+    sub_n = gad.with_subspace(base_n, torch.from_numpy(basis), encoding_axis=-3)
+    b = torch.from_numpy(_c(rng, C, *grid))
+    xk = torch.from_numpy(_c(rng, K, *img))
+    rec = dict(
+        in_mask=mask, in_density=density, in_smaps=smaps, in_basis=basis, in_b=b.numpy(), in_xk=xk.numpy(),
+        meta=np.array([repr(("submasked", grid, img, C, K, T))]),
+        ref_sub_adjoint=sub_t.adjoint(b).numpy(),
+        ref_sub_forward=sub_t.forward(xk).numpy(),
+        ref_sub_normal_toep=sub_t.normal(xk).numpy(),
+        ref_sub_normal_notoep=sub_n.normal(xk).numpy(),
+    )
+    rec["ref_sub_psf"] = sub_t._toep_op.psf.numpy()
+    rec["ref_sub_cg"] = sub_t.solve(b, method="cg", max_iter=8, damp=1e-3, tol=0.0).numpy()
+    np.savez_compressed(out / "sub_masked.npz", **rec)
+    print("wrote submasked")
+
+
 def main():
     pg = refimport.import_reference()
     torch.set_num_threads(4)
@@ -248,6 +286,8 @@ def main():
         make_operator_cases(pg, out)
     if not only or "subspace" in only:
         make_subspace_cases(pg, out)
+    if not only or "submasked" in only:
+        make_subspace_masked_case(pg, out)
 
 
 if __name__ == "__main__":

@@ -171,3 +171,24 @@ def test_oracle_subspace_matches_reference():
     AHb = oo.sub_adjoint(b, idx, sw, tidx, B, gs, img, sm)
     x = oo.cg(lambda v: oo.sub_toeplitz_normal(v, P, gs, img, sm), AHb, damp=1e-3, max_iter=6)
     assert rel_l2(x, z["ref_sub_cg"]) < 1e-4
+
+
+def test_oracle_subspace_masked_matches_reference():
+    """SubspaceMaskedFFT on a (T, gy, gx) grid with T = 5 frames on axis 0."""
+    z = golden("sub_masked.npz")
+    _, grid, img, C, K, T = parse_meta(z["meta"])
+    sm = z["in_smaps"].astype(np.complex128)
+    B = z["in_basis"].astype(np.complex128)
+    mask = z["in_mask"].astype(np.float64)
+    b = z["in_b"].astype(np.complex128)
+    xk = z["in_xk"].astype(np.complex128)
+    adj = oo.submasked_adjoint(b, mask, B, 0, grid, img, sm)
+    assert rel_l2(adj, z["ref_sub_adjoint"]) < 1e-5
+    assert rel_l2(oo.submasked_forward(xk, mask, B, 0, grid, img, sm), z["ref_sub_forward"]) < 1e-5
+    P = oo.submasked_psf(z["in_density"].astype(np.float64), B, 0, grid)
+    assert rel_l2(P, z["ref_sub_psf"]) < 1e-5
+    assert rel_l2(oo.sub_toeplitz_normal(xk, P, grid, img, sm), z["ref_sub_normal_toep"]) < 1e-5
+    nested = oo.submasked_adjoint(oo.submasked_forward(xk, mask, B, 0, grid, img, sm), mask, B, 0, grid, img, sm)
+    assert rel_l2(nested, z["ref_sub_normal_notoep"]) < 1e-5
+    x = oo.cg(lambda v: oo.sub_toeplitz_normal(v, P, grid, img, sm), adj, damp=1e-3, max_iter=8)
+    assert rel_l2(x, z["ref_sub_cg"]) < 1e-4
