@@ -81,6 +81,29 @@ def test_cg_and_lsmr_match_reference(cuda, name):
     assert op.toeplitz is True and opn.toeplitz is False
 
 
+def test_cg_with_a_preconditioner_object(cuda):
+    """``preconditioner=`` takes any object with ``.apply(r)`` (``_solvers.py:115, 133``)
+    and runs the host-driven loop; a scalar preconditioner leaves the CG
+    iterates unchanged, so the result equals the unpreconditioned solve and
+    the reference's."""
+
+    class Scaled:
+        calls = 0
+
+        def apply(self, r):
+            Scaled.calls += 1
+            return 0.37 * r
+
+    z, g, C = _plan("op2d", cuda)
+    op = SparseFFT(plan=g.plan, smaps=torch.from_numpy(z["in_smaps"]), toeplitz=True)
+    bn = torch.from_numpy(z["in_b"]).reshape(C, *op.natural_shape)
+    x = op.solve(bn, method="cg", max_iter=8, damp=1e-3, tol=0.0, preconditioner=Scaled())
+    assert Scaled.calls == 9  # once before the loop and once per iteration
+    assert rel_l2(x.numpy(), z["ref_cg"]) < 1e-4
+    x0 = op.solve(bn, method="cg", max_iter=8, damp=1e-3, tol=0.0)
+    assert rel_l2(x.numpy(), x0.numpy()) < 1e-5
+
+
 def test_device_lsmr_graph_eager_and_early_stop(cuda):
     """Device LSMR: the graph-replayed iteration and the eager loop agree; a
     stopping tolerance freezes the state at the iteration where the
