@@ -354,7 +354,7 @@ PGB_API int pgb_grog_tc_wait_limit(int64_t limit, int64_t* previous);
  * tensor memory (M = 128 replicas per tile).  bf16x3 products, FP32
  * accumulation.  C = 12 or 32 coils.  x, out: (2C, R) float realified
  * (row 2c real part of coil c, 2c + 1 imaginary); idx: R int32
- * i | j << 8 | k << 16, each < 11; W: (4, 2C, 2C) float realified
+ * i | j << 8 | k << 16, each < 11 (a larger byte reads step 10); W: (4, 2C, 2C) float realified
  * [stage][output][input]; ph: (3, 11, C) complex64 phases.  rep >= 1 applies
  * the chain rep times per loaded tile.  timeouts: int32 device counter
  * (required for variant 1), incremented by every CTA whose bounded tensor-core

@@ -23,7 +23,8 @@
 //
 // Both compute bf16x3 products (hi*hi + hi*lo + lo*hi) with FP32 accumulation.
 // Layouts: x and out (2C, R) float, realified (row 2c = Re of coil c, 2c + 1 =
-// Im); idx int32 per replica, i | j << 8 | k << 16 (each < kSteps); W (4, 2C,
+// Im); idx int32 per replica, i | j << 8 | k << 16 (each < kSteps, larger bytes
+// read step kSteps - 1); W (4, 2C,
 // 2C) float, realified [stage][output][input]; ph (3, kSteps, C) float2.
 // rep > 1 applies the chain rep times per loaded tile, so that the chain's
 // time can be separated from the loads and stores.  Every mbarrier wait is
@@ -56,6 +57,10 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint3
   hi = *reinterpret_cast<const uint32_t*>(&h);
   lo = bf2_bits(a - hf.x, b - hf.y);
 }
+// Shift step of stage s packed in byte s of a replica's index word, clamped to
+// the table (a caller's out-of-range byte reads the last step, never past the
+// shared-memory phase table).
+__device__ __forceinline__ int step_of(int packed, int s) { return min((packed >> (8 * s)) & 0xFF, kSteps - 1); }
 __device__ __forceinline__ void cmul_inplace(float& re, float& im, float2 p) {
   const float r = re * p.x - im * p.y;
   im = re * p.y + im * p.x;
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(128) chain_tcgen05_kernel(const float* __restr
 #pragma unroll
         for (int k = 0; k < KP; ++k) v[k] = __uint_as_float(u[k]);
         if (s < 3) {
-          const float2* prow = phs + (s * kSteps + ((pi >> (8 * s)) & 0xFF)) * L::PHS;
+          const float2* prow = phs + (s * kSteps + step_of(pi, s)) * L::PHS;
 #pragma unroll
           for (int c = 0; c < C; ++c) cmul_inplace(v[2 * c], v[2 * c + 1], prow[c]);
         }
@@ -376,8 +381,8 @@ __global__ void __launch_bounds__(256) chain_mma_kernel(const float* __restrict_
 #pragma unroll
           for (int e = 0; e < 4; ++e) acc[j][e] = d[j][e];
         if (s < 3) {
-          const float2* q0 = phs + (s * kSteps + ((p0 >> (8 * s)) & 0xFF)) * L::PHS;
-          const float2* q1 = phs + (s * kSteps + ((p1 >> (8 * s)) & 0xFF)) * L::PHS;
+          const float2* q0 = phs + (s * kSteps + step_of(p0, s)) * L::PHS;
+          const float2* q1 = phs + (s * kSteps + step_of(p1, s)) * L::PHS;
 #pragma unroll
           for (int j = 0; j < NT; ++j) {  // columns 2t, 2t + 1 of n-tile j: coil 4 j + t
             cmul_inplace(acc[j][0], acc[j][1], q0[4 * j + t]);
