@@ -473,6 +473,11 @@ PGB_API int pgb_dot_f64(const void* a, const void* b, int64_t n, void* scratch, 
 /* alpha = rz_old / (pAp + 1e-30); x += alpha p; r -= alpha Ap */
 PGB_API int pgb_cg_update_xr(void* x, void* r, const void* p, const void* Ap, int64_t n,
                              const void* scalars, void* stream);
+/* pgb_cg_update_xr followed by pgb_dot_f64(r, NULL, mode 1) in one pass:
+ * x += alpha p; r -= alpha Ap; rr = |r|^2 (FP64), rel, done.  Uses the
+ * scratch's first counter, as pgb_dot_f64 does. */
+PGB_API int pgb_cg_update_xr_rr(void* x, void* r, const void* p, const void* Ap, int64_t n, void* scalars,
+                                void* scratch, void* stream);
 /* beta = rr / (rz_old + 1e-30); p = r + beta p; rz_old = rr */
 PGB_API int pgb_cg_update_p(void* p, const void* r, int64_t n, void* scalars, void* scratch,
                             void* stream);
@@ -486,6 +491,8 @@ PGB_API int pgb_dot_f64_batched(const void* a, const void* b, int64_t n, int64_t
                                 void* scalars, int out_slot, int mode, void* stream);
 PGB_API int pgb_cg_update_xr_batched(void* x, void* r, const void* p, const void* Ap, int64_t n,
                                      int64_t frames, const void* scalars, void* stream);
+PGB_API int pgb_cg_update_xr_rr_batched(void* x, void* r, const void* p, const void* Ap, int64_t n,
+                                        int64_t frames, void* scalars, void* scratch, void* stream);
 PGB_API int pgb_cg_update_p_batched(void* p, const void* r, int64_t n, int64_t frames, void* scalars,
                                     void* scratch, void* stream);
 /* y += a x */

@@ -101,6 +101,7 @@ _SIGS = {
     "pgb_fft_shift": [_vp, _vp, _vp, _i64, _i32, _vp, _f32, _i32, _vp],
     "pgb_dot_f64": [_vp, _vp, _i64, _vp, _vp, _i32, _i32, _vp],
     "pgb_cg_update_xr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp],
+    "pgb_cg_update_xr_rr": [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_cg_update_p": [_vp, _vp, _i64, _vp, _vp, _vp],
     "pgb_axpy": [_vp, _vp, _f32, _i64, _vp],
     "pgb_grog_grid_v8": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],
@@ -110,6 +111,7 @@ _SIGS = {
     "pgb_psf_apply_kk": [_vp, _vp, _i64, _i64, _i64, _i64, _vp],
     "pgb_dot_f64_batched": [_vp, _vp, _i64, _i64, _vp, _vp, _i32, _i32, _vp],
     "pgb_cg_update_xr_batched": [_vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp],
+    "pgb_cg_update_xr_rr_batched": [_vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp],
     "pgb_cg_update_p_batched": [_vp, _vp, _i64, _i64, _vp, _vp, _vp],
     "pgb_dot_f64_noalloc": [_vp, _vp, _i64, _i64, _vp, _vp],
     "pgb_grog_grid_v6": [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _i64, _vp, _vp],

@@ -94,10 +94,9 @@ class DeviceCG:
         self.op._normal_into(self.p, self.Ap, self.damp)
         _lib.call("pgb_dot_f64", self.p.data_ptr(), self.Ap.data_ptr(), self.n, self.scratch.data_ptr(),
                   self.scal.data_ptr(), 1, 0, st)
-        _lib.call("pgb_cg_update_xr", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
-                  self.Ap.data_ptr(), self.n, self.scal.data_ptr(), st)
-        _lib.call("pgb_dot_f64", self.r.data_ptr(), None, self.n, self.scratch.data_ptr(),
-                  self.scal.data_ptr(), 2, 1, st)
+        # x, r update and rr = |r|^2 with the residual check, one pass
+        _lib.call("pgb_cg_update_xr_rr", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
+                  self.Ap.data_ptr(), self.n, self.scal.data_ptr(), self.scratch.data_ptr(), st)
         _lib.call("pgb_cg_update_p", self.p.data_ptr(), self.r.data_ptr(), self.n, self.scal.data_ptr(),
                   self.scratch.data_ptr(), st)
 
@@ -189,10 +188,8 @@ class BatchedDeviceCG:
         self.op._normal_frames_into(self.p, self.Ap, self.damp)
         _lib.call("pgb_dot_f64_batched", self.p.data_ptr(), self.Ap.data_ptr(), self.n, F,
                   self.scratch.data_ptr(), self.scal.data_ptr(), 1, 0, st)
-        _lib.call("pgb_cg_update_xr_batched", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
-                  self.Ap.data_ptr(), self.n, F, self.scal.data_ptr(), st)
-        _lib.call("pgb_dot_f64_batched", self.r.data_ptr(), None, self.n, F, self.scratch.data_ptr(),
-                  self.scal.data_ptr(), 2, 1, st)
+        _lib.call("pgb_cg_update_xr_rr_batched", self.x.data_ptr(), self.r.data_ptr(), self.p.data_ptr(),
+                  self.Ap.data_ptr(), self.n, F, self.scal.data_ptr(), self.scratch.data_ptr(), st)
         _lib.call("pgb_cg_update_p_batched", self.p.data_ptr(), self.r.data_ptr(), self.n, F,
                   self.scal.data_ptr(), self.scratch.data_ptr(), st)
 

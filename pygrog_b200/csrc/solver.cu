@@ -134,6 +134,63 @@ __global__ void cg_update_xr_kernel(float2* __restrict__ x, float2* __restrict__
   }
 }
 
+// x += alpha p ; r -= alpha Ap, and in the same pass rr = |r|^2 in FP64 with
+// the residual check of dot_f64 mode 1 (rel = sqrt(rr) / r0, done |= rel < tol):
+// one launch and one read of r fewer per iteration than update + dot.  At most
+// kRedBlocks blocks (their partials go to scratch; the first counter).
+__global__ void __launch_bounds__(kRedThreads) cg_update_xr_rr_kernel(float2* __restrict__ x,
+                                                                      float2* __restrict__ r,
+                                                                      const float2* __restrict__ p,
+                                                                      const float2* __restrict__ Ap, int64_t n,
+                                                                      double* __restrict__ scal,
+                                                                      double* __restrict__ scratch) {
+  {
+    const int64_t f = blockIdx.y;
+    x += f * n;
+    r += f * n;
+    p += f * n;
+    Ap += f * n;
+    scal += f * kScalars;
+    scratch += f * kScratchWords;
+  }
+  if (scal[S_DONE] != 0.0) return;  // grid-uniform: converged, skip
+  const float alpha = static_cast<float>(scal[S_RZ] / (scal[S_PAP] + 1e-30));
+  double acc = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float2 pv = p[i], av = Ap[i];
+    float2 xv = x[i], rv = r[i];
+    xv.x = fmaf(alpha, pv.x, xv.x);
+    xv.y = fmaf(alpha, pv.y, xv.y);
+    rv.x = fmaf(-alpha, av.x, rv.x);
+    rv.y = fmaf(-alpha, av.y, rv.y);
+    x[i] = xv;
+    r[i] = rv;
+    acc += static_cast<double>(rv.x) * rv.x + static_cast<double>(rv.y) * rv.y;
+  }
+  const double s = block_sum(acc);
+  __shared__ bool last;
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + kRedBlocks);
+  if (threadIdx.x == 0) {
+    scratch[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += blockDim.x) t += scratch[i];
+  t = block_sum(t);
+  if (threadIdx.x == 0) {
+    scal[S_RR] = t;
+    const double rel = sqrt(t) / scal[S_R0];
+    scal[S_REL] = rel;
+    if (rel < scal[S_TOL]) scal[S_DONE] = 1.0;
+    *counter = 0u;
+  }
+}
+
 // p = r + beta p  with beta = rr / (rz_old + 1e-30); the last block then
 // commits rz_old = rr for the next iteration (grid-wide ordering through a
 // completion counter in scratch).
@@ -215,6 +272,25 @@ int pgb_cg_update_xr(void* x, void* r, const void* p, const void* Ap, int64_t n,
       static_cast<float2*>(x), static_cast<float2*>(r), static_cast<const float2*>(p),
       static_cast<const float2*>(Ap), n, static_cast<const double*>(scalars));
   PGB_LAUNCH_CHECK("cg_update_xr");
+  return PGB_OK;
+}
+
+int pgb_cg_update_xr_rr(void* x, void* r, const void* p, const void* Ap, int64_t n, void* scalars, void* scratch,
+                        void* stream) {
+  return pgb_cg_update_xr_rr_batched(x, r, p, Ap, n, 1, scalars, scratch, stream);
+}
+
+int pgb_cg_update_xr_rr_batched(void* x, void* r, const void* p, const void* Ap, int64_t n, int64_t frames,
+                                void* scalars, void* scratch, void* stream) {
+  clear_error();
+  PGB_REQUIRE(n >= 0 && frames >= 0 && frames <= 65535, PGB_ERR_INVALID, "cg_update_xr_rr: invalid sizes");
+  if (n == 0 || frames == 0) return PGB_OK;
+  PGB_REQUIRE(x && r && p && Ap && scalars && scratch, PGB_ERR_INVALID, "cg_update_xr_rr: null pointer");
+  const dim3 grid(grid_for(n, kRedThreads, kRedBlocks), static_cast<unsigned>(frames));
+  cg_update_xr_rr_kernel<<<grid, kRedThreads, 0, as_stream(stream)>>>(
+      static_cast<float2*>(x), static_cast<float2*>(r), static_cast<const float2*>(p),
+      static_cast<const float2*>(Ap), n, static_cast<double*>(scalars), static_cast<double*>(scratch));
+  PGB_LAUNCH_CHECK("cg_update_xr_rr");
   return PGB_OK;
 }
 
