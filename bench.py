@@ -524,6 +524,9 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
         torch.cuda.empty_cache()
     wall, lanes_best, t_capture = best
     sc = sum(p.C * int(np.prod(p.spatial)) for p in protos.values())
+    cg_bytes = sum(p.max_iter * _cg_iter_bytes(int(np.prod(p.op.grid_shape)), int(np.prod(p.image_shape)), p.C)
+                   for p in protos.values())
+    peak, _ = _peaks()
     # the per-request path on 4 streams, for comparison
     server = ReconServer(protos, mem_budget=150 << 30, max_batch=1, n_slots=4, device=dev)
     data = {k: h for k, h in zip(protos, host_in)}
@@ -536,10 +539,23 @@ def c3_batch(dev, n_slices: int = 64, seed: int = 1004) -> dict:
     return {"slices": n_slices, "ms_per_batch": wall * 1e3, "lanes": lanes_best, "ms_by_lanes": by_lanes,
             "sample_coils": sc,
             "sample_coils_per_s": sc / wall, "recons_per_s": n_slices / wall, "cg_iters": 20,
+            "cg_bytes": cg_bytes, "cg_gbs": cg_bytes / wall / 1e9, "cg_roofline_frac": cg_bytes / wall / 1e9 / peak,
             "setup_s": t_proto + t_capture, "protocols_s": t_proto, "capture_s": t_capture,
             "protocol_ms_per_slice": t_proto * 1e3 / n_slices,
             "per_request_streams_ms": min(prev[1:]) * 1e3, "mode": "one graph, slices as branches",
             "note": "wall time incl. host<->device copies; plans, tables, PSFs and the graph built in setup"}
+
+
+def _cg_iter_bytes(G: int, img: int, C: int) -> int:
+    """Algorithmic bytes of one CG iteration on the Toeplitz normal operator:
+    coil expansion into the (padded) grid, the forward and inverse 2-D FFTs as
+    two passes of read + write each, the PSF multiply, the crop + SENSE
+    combine, and the CG vectors (dots and updates)."""
+    grid_b = C * G * 8
+    return (img * 8 + C * img * 8 + grid_b  # expand: x, maps in, padded coil grid out
+            + 4 * grid_b + 2 * grid_b + G * 4 + 4 * grid_b  # FFT (2 passes), PSF (r + w, PSF), IFFT
+            + 2 * C * img * 8 + 2 * img * 8  # crop + combine (coil images, maps), damp add
+            + 8 * img * 8)  # CG: the dots and the x / r / p updates
 
 
 def cg_sense_c2(dev, iters: int = 30) -> dict:
@@ -581,11 +597,7 @@ def cg_sense_c2(dev, iters: int = 30) -> dict:
     G = int(np.prod(p.op.grid_shape))
     img = int(np.prod(p.image_shape))
     C = p.C
-    grid_b = C * G * 8
-    iter_bytes = (img * 8 + C * img * 8 + grid_b  # expand: x, maps in, padded coil grid out
-                  + 4 * grid_b + 2 * grid_b + G * 4 + 4 * grid_b  # FFT (2 passes), PSF (r + w, PSF), IFFT
-                  + 2 * C * img * 8 + 2 * img * 8  # crop + combine (coil images, maps), damp add
-                  + 8 * img * 8)  # CG: two FP64 dots and the x / r / p updates
+    iter_bytes = _cg_iter_bytes(G, img, C)
     peak, _ = _peaks()
     gbs = iter_bytes / (ms_iter / 1e3) / 1e9
     return {"ms_per_recon": ms, "ms_per_iter": ms_iter, "cg_iters": p.max_iter, "coils": C,
@@ -793,8 +805,8 @@ def _compact_sections(coilc, cg2, c3, serving, tune):
 
     out["coil_compress_c1"] = pick(coilc, ("tc_ms", "tc_gbs", "tc_frac", "fp32_ms", "tc_rel_err_vs_fp32"))
     out["cg_sense_c2"] = pick(cg2, ("ms_per_recon", "ms_per_iter", "iter_gbs", "iter_roofline_frac"))
-    out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "protocol_ms_per_slice", "capture_s",
-                                "per_request_streams_ms"))
+    out["c3_batch"] = pick(c3, ("ms_per_batch", "recons_per_s", "cg_roofline_frac", "protocol_ms_per_slice",
+                                "capture_s", "per_request_streams_ms"))
     if isinstance(serving, dict) and "error" not in serving:
         o = serving.get("open_loop", {})
         out["serving"] = {k: _r(serving.get(k)) for k in ("closed_loop_recons_per_s", "single_instance_recons_per_s",
