@@ -40,7 +40,9 @@ class UnevenBatch:
     number of parallel chains in the graph (default: one per protocol).  Inputs go in
     :attr:`host_in` (page-locked, one ``(C, *spatial)`` tensor per protocol),
     :meth:`run` launches the graph and returns :attr:`host_out` (page-locked
-    ``image_shape`` tensors).
+    ``image_shape`` tensors).  The graph copies from and to these very
+    tensors: write into them, and replace them (other page-locked tensors of
+    the same shapes) only before the graph is captured.
     """
 
     def __init__(self, protocols, device=None, lanes: int | None = None):
@@ -113,6 +115,7 @@ class UnevenBatch:
             if gc_on:
                 gc.enable()
         self.graph = g
+        self._bound = ([id(t) for t in self.host_in], [id(t) for t in self.host_out])
 
     def run(self, inputs=None, sync: bool = True) -> list:
         """Reconstruct the batch.  ``inputs`` (optional): one ``(C, *spatial)``
@@ -124,6 +127,9 @@ class UnevenBatch:
                 dst.copy_(torch.as_tensor(src))
         if self.graph is None:
             self.capture()
+        elif self._bound != ([id(t) for t in self.host_in], [id(t) for t in self.host_out]):
+            raise RuntimeError("UnevenBatch: host_in / host_out were replaced after the graph was captured; "
+                               "copy into the captured tensors instead")
         self.graph.replay()
         if sync:
             torch.cuda.current_stream(self.device).synchronize()
