@@ -682,14 +682,11 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
   while (true) {
     const bool more = st.p + 1 < p1;
     if (more) {
-      stage_x(st.d1, u1, xs0 + (buf ^ 1) * lay.xs_sz);
-      stage_meta(meta, wts, st.d1, cap, ms0 + (buf ^ 1) * cap, ws0 + (buf ^ 1) * cap);
-      commit();
       if (st.p + 2 < p1) {
         prefetch_x(st.d2, u2);
         prefetch_meta(meta, wts, st.d2, cap);
       }
-      wait_groups<1>();
+      wait_groups<0>();  // sub-chunk p's copies (issued during iteration p - 1)
     } else {
       wait_groups<0>();
     }
@@ -700,10 +697,11 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       const float2* xs = xs0 + buf * lay.xs_sz;
       const int2* msb = ms0 + buf * cap;
       const float* wsb = ws0 + buf * cap;
-      if (warp * 16 < nr) {  // warp-uniform: m-tiles warp (and warp + 8 up to 16 coils)
-        constexpr int NTL = Shape<CP>::NTL;
-        Row rw[NTL][2];
-        float2 v[NTL][2][NT];
+      constexpr int NTL = Shape<CP>::NTL;
+      Row rw[NTL][2];
+      float2 v[NTL][2][NT];
+      const bool act = warp * 16 < nr;  // warp-uniform: m-tiles warp (and warp + 8 up to 16 coils)
+      if (act) {
 #pragma unroll
         for (int T = 0; T < NTL; ++T)
 #pragma unroll
@@ -718,6 +716,16 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
             }
           }
         chain<CP, NS, TERMS, false>(v, wsm, dtl, nsteps, ph.stride, rw, lane);
+      }
+      // the next sub-chunk's copies go out between the chain and the row sums:
+      // issued at the top of the iteration they competed with the chain's
+      // shared-memory traffic for the load/store pipe (1.4% slower at 192^3)
+      if (more) {
+        stage_x(st.d1, u1, xs0 + (buf ^ 1) * lay.xs_sz);
+        stage_meta(meta, wts, st.d1, cap, ms0 + (buf ^ 1) * cap, ws0 + (buf ^ 1) * cap);
+        commit();
+      }
+      if (act) {
 #pragma unroll
         for (int T = 0; T < NTL; ++T) {
           if ((warp + 8 * T) * 16 >= nr) break;  // warp-uniform
