@@ -470,3 +470,30 @@ def test_device_power_path_matches_host_powers_on_near_singular_operators():
         P = _grappa.grappa_power_device(G, d)
         assert rel_l2(P.numpy(), _grappa.grappa_power(G, d).numpy()) < 1e-12
         assert rel_l2(P[d.numel() - 1].numpy() @ P[d.numel() - 1].numpy(), G.numpy()) < 1e-10  # G^0.5 G^0.5
+
+
+def test_chain_operands_realify_the_complex_matrices():
+    """The shift chain's realified matrices ([stage][output][input], rows 2c / 2c + 1
+    the real / imaginary part of coil c) apply the complex operators, and the
+    packed shift index holds (i, j, k) in bytes 0 / 1 / 2."""
+    from pygrog_b200.calib import _chain
+
+    rng = np.random.default_rng(8)
+    C = 12
+    W = rng.standard_normal((4, C, C)) + 1j * rng.standard_normal((4, C, C))
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, (3, _chain.STEPS, C)))
+    Wr, phr = _chain.chain_operands(W, ph, "cpu")
+    assert tuple(Wr.shape) == (4, 2 * C, 2 * C) and Wr.dtype == torch.float32
+    assert tuple(phr.shape) == (3, _chain.STEPS, C, 2)
+    x = rng.standard_normal(C) + 1j * rng.standard_normal(C)
+    xr = np.empty(2 * C)
+    xr[0::2], xr[1::2] = x.real, x.imag
+    for s in range(4):
+        y = Wr[s].double().numpy() @ xr
+        np.testing.assert_allclose(y[0::2] + 1j * y[1::2], W[s] @ x, rtol=1e-5, atol=1e-5)
+    ijk = torch.tensor([[3, 0, 10], [7, 10, 1], [10, 5, 0]])
+    packed = _chain.pack_shift_indices(ijk)
+    assert packed.dtype == torch.int32
+    for r in range(3):
+        p = int(packed[r])
+        assert (p & 0xFF, (p >> 8) & 0xFF, (p >> 16) & 0xFF) == tuple(int(v) for v in ijk[:, r])
