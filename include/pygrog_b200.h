@@ -239,7 +239,11 @@ PGB_API int pgb_grog_degrid(const void* grid, int64_t G, void* out, int64_t N,
  *               a sub-chunk (at most sub_cap <= 512 slots / replicas each)
  *   meta[]      int2 {cell | slot << 16, inner | outer << 16} per replica
  *   w[]         float weight per replica
- *   zero_bricks bricks the forward writes with zeros first (empty + split)
+ *   zero_bricks bricks the forward writes with zeros first (empty + split);
+ *               the last n_empty_tail of them are empty bricks (no
+ *               sub-chunk touches them), which the tensor-core forward on
+ *               its tensor-copy path clears from inside its kernel while
+ *               it grids (0: every listed brick is cleared beforehand)
  * inner_lc / outer_lc (forward) and inner_h_lc / outer_h_lc (adjoint): the
  * factors (inner = whole table when n_outer == 1; outer unused then) in
  * lane-chunk layout, entry (q, j, l, t) = M[q][l*RPL + t][j] with RPL = 2
@@ -266,6 +270,7 @@ typedef struct pgb_v6_plan {
    * it; a head starts a segment of entries of one cell (summed by one thread),
    * shared marks segments of a cell that has several (added atomically) */
   const int32_t* cword;
+  int32_t n_empty_tail;
 } pgb_v6_plan;
 
 PGB_API size_t pgb_grog_v6_smem_bytes(int64_t C, int64_t cells, int64_t n_inner, int64_t n_outer,

@@ -49,6 +49,7 @@ class V6PlanC(ctypes.Structure):
         ("zero_bricks", _vp),
         ("n_zero_bricks", ctypes.c_int32),
         ("cword", _vp),
+        ("n_empty_tail", ctypes.c_int32),
     ]
 
 

@@ -690,9 +690,21 @@ class GrogGridder:
             if self.mode in ("v6", "v8", "tc", "tc1"):
                 return 1 + (1 if self.plan2 is not None else 0) + (1 if self.adj_plan.zero_src.numel() else 0)
             return 1 + (1 if (not bp.multi and bp.zero_src.numel()) else 0)
+        if self.mode in ("tc", "tc1") and self._tile_copies():
+            return 1 + (1 if bp.zero_bricks.numel() > bp.n_empty_tail else 0)
         if self.mode in ("v6", "v8", "tc", "tc1"):
             return 1 + (1 if bp.zero_bricks.numel() else 0)
         return 1 + (1 if bp.split_bricks.numel() else 0)
+
+    def _tile_copies(self) -> bool:
+        """Whether the tensor-core kernels move brick tiles by tensor copies
+        (the launcher's test: coil count a kernel width, even grid and brick
+        width, copies switched on); their forward then clears empty bricks
+        inside the gridding kernel."""
+        C = self.C
+        width = (C + 3) // 4 * 4 if C <= 16 else (C + 7) // 8 * 8
+        gx, bx = self.plan.grid[-1], self.plan.brick[-1]
+        return C == width and gx % 2 == 0 and bx % 2 == 0 and _lib.lib().pgb_grog_tc_use_tma(-1) == 1
 
     def _outer_ptr(self, h: bool):
         t = self.outer_h if h else self.outer

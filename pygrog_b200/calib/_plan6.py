@@ -51,7 +51,8 @@ class BrickPlan6:
       ``n_pad``  padding entries (``lane_order`` only: meta ``-1``, weight 0,
                  cell order cell = ``cells``) that round every sub-chunk to
                  whole quarter-warps
-      ``zero_bricks`` bricks the forward zeroes first (empty and split)
+      ``zero_bricks`` bricks the forward zeroes (split ones, then the
+      ``n_empty_tail`` empty ones)
       ``zero_src`` samples with no replica in this plan; ``multi`` whether a
       sample has more than one.
     """
@@ -329,7 +330,13 @@ class BrickPlan6:
                          else np.zeros(n_cta))
         split_b = nit_b > 1
         self.split_bricks = torch.nonzero(split_b).squeeze(1).to(torch.int32).contiguous()
-        self.zero_bricks = torch.nonzero(split_b | (cnt == 0)).squeeze(1).to(torch.int32).contiguous()
+        # split bricks first (cleared before the gridding kernel: they take
+        # reduce-adds), then the empty ones (cleared by the tensor-core
+        # forward's CTAs while they grid, or beforehand by the other kernels)
+        empty_b = cnt == 0
+        self.zero_bricks = torch.cat([torch.nonzero(split_b & ~empty_b), torch.nonzero(empty_b)]).squeeze(1)
+        self.zero_bricks = self.zero_bricks.to(torch.int32).contiguous()
+        self.n_empty_tail = int(empty_b.sum())
         per_src = torch.bincount(src[src >= 0], minlength=n_src)
         self.multi = bool(int(per_src.max()) > 1) if per_src.numel() else False
         self.zero_src = torch.nonzero(per_src == 0).squeeze(1).to(torch.int32).contiguous()
@@ -346,7 +353,7 @@ class BrickPlan6:
         return _lib.V6PlanC(
             ptr(self.sd), ptr(self.si), self.cta_ptr.data_ptr(), self.n_cta if self.sd.numel() else 0,
             ptr(self.uniq), ptr(self.meta), ptr(self.w), self.sub_cap, gz, gy, gx, bz, by, bx, nbz, nby, nbx,
-            ptr(self.zero_bricks), int(self.zero_bricks.numel()), ptr(self.cword),
+            ptr(self.zero_bricks), int(self.zero_bricks.numel()), ptr(self.cword), self.n_empty_tail,
         )
 
 

@@ -54,6 +54,7 @@ namespace tc {
 
 constexpr int kT = 256;  // threads per CTA: 8 warps x 2 m-tiles = 256 replicas per sub-chunk (128 above 16 coils)
 constexpr int kFirst = 1, kLast = 2, kSplit = 4;
+constexpr int kZeroPerFlush = 4;  // forward: clearing stores of empty bricks per brick item
 
 // 16-byte groups of B-fragment words per n-tile (head or tail) for CP coils:
 // ceil((2 * k16 chunks + k8 chunk) / 4), k16 = CP / 8, k8 = (CP / 4) % 2
@@ -607,11 +608,25 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     const uint32_t* __restrict__ wfrag, const float2* __restrict__ dtab, int nsteps, const int4* __restrict__ sd,
     const int2* __restrict__ si, const int32_t* __restrict__ cta_ptr, const int32_t* __restrict__ uniq,
     const int2* __restrict__ meta, const float* __restrict__ wts, int cap, Geom geom,
-    const __grid_constant__ CUtensorMap tmap) {
+    const __grid_constant__ CUtensorMap tmap, const int32_t* __restrict__ zempty, int n_empty) {
   extern __shared__ __align__(128) float4 smem4[];
   constexpr int NT = Shape<CP>::NT, TS = Shape<CP>::TS;
   const int p0 = cta_ptr[blockIdx.x], p1 = cta_ptr[blockIdx.x + 1];
   if (p0 >= p1) return;  // block-uniform
+  // bricks no sub-chunk touches (zempty, tensor-copy path only): this CTA
+  // clears a share proportional to its sub-chunks by storing its tile while
+  // the tile is clear (at the first sub-chunk of each brick item), at most
+  // kZeroPerFlush per item and the rest when it is done, so that the
+  // clearing writes overlap the chains.  Thread 0 keeps the position in the
+  // list (z_next); every thread the count left (zleft).
+  __shared__ int z_next;
+  int zleft = 0;
+  if (TMA && n_empty > 0) {
+    const int64_t P = cta_ptr[gridDim.x];
+    const int z0 = static_cast<int>(static_cast<int64_t>(n_empty) * p0 / P);
+    zleft = static_cast<int>(static_cast<int64_t>(n_empty) * p1 / P) - z0;
+    if (threadIdx.x == 0) z_next = z0;
+  }
   const int cells = geom.bz * geom.by * geom.bx;
   const Smem lay(CP, NS, nsteps, cells, cap, true, TMA);
   const Phases ph(CP, NS, nsteps);
@@ -677,6 +692,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
   stage_w<CP, NS>(reinterpret_cast<uint32_t*>(wsm), wfrag);
   stage_phases(dt, dtab, CP, NS, nsteps, ph);
   for (int i = tid; i < lay.tile_sz; i += kT) tile[i] = make_float2(0.f, 0.f);
+  if (TMA) fence_proxy_async();  // the cleared tile -> visible to tensor-copy stores
 
   int buf = 0;
   while (true) {
@@ -692,6 +708,20 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     }
     const int u3 = ld_u(st.d3, st.p + 3 < p1);
     __syncthreads();  // staging buffer `buf` complete; tile zeroed / flushed
+    // block-uniform; an item's first sub-chunk follows a flush (or the start)
+    const int zn = (TMA && (st.i0.y & kFirst)) ? min(kZeroPerFlush, zleft) : 0;
+    if (TMA && zn > 0) {
+      if (tid == 0) {
+        const int z = z_next;
+        for (int k = 0; k < zn; ++k) {
+          int z0, y0, x0;
+          origin(geom, __ldg(zempty + z + k), z0, y0, x0);
+          tma_store_tile(&tmap, 2 * x0, y0, z0, b * C, tile, false);
+        }
+        z_next = z + zn;
+      }
+      zleft -= zn;
+    }
     {
       const int nr = n_reps(st.d0, cap), nu = n_slots(st.d0, cap);
       const float2* xs = xs0 + buf * lay.xs_sz;
@@ -725,6 +755,10 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
         stage_meta(meta, wts, st.d1, cap, ms0 + (buf ^ 1) * cap, ws0 + (buf ^ 1) * cap);
         commit();
       }
+      if (TMA && zn > 0) {  // the clearing stores have read the tile before it takes row sums
+        if (tid == 0) bulk_wait_read_all();
+        __syncthreads();
+      }
       if (act) {
 #pragma unroll
         for (int T = 0; T < NTL; ++T) {
@@ -750,6 +784,7 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
       __syncthreads();
       float4* t4 = reinterpret_cast<float4*>(tile);
       for (int i = tid; i < (C * cells) / 2; i += kT) t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (zleft > 0) fence_proxy_async();  // the cleared tile -> visible to the clearing stores
     } else if (st.i0.y & kLast) {
       int z0, y0, x0;
       origin(geom, st.i0.x, z0, y0, x0);
@@ -783,6 +818,15 @@ __global__ void __launch_bounds__(kT, Regs<CP, NS>::MINB) grog_grid_tc_kernel(
     u1 = u2;
     u2 = u3;
     buf ^= 1;
+  }
+  if (TMA && zleft > 0 && (st.i0.y & kLast)) {  // the last sub-chunk flushed its brick: the tile is clear
+    __syncthreads();
+    if (tid == 0)
+      for (int k = z_next; k < z_next + zleft; ++k) {
+        int z0, y0, x0;
+        origin(geom, __ldg(zempty + k), z0, y0, x0);
+        tma_store_tile(&tmap, 2 * x0, y0, z0, b * C, tile, false);
+      }
   }
   if (TMA && tid == 0) bulk_wait_all();
 }
@@ -1155,20 +1199,26 @@ int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const v
   const int cells = plan->bz * plan->by * plan->bx;
   const size_t smem = pgb_grog_tc_smem_bytes(C, cells, nsteps, ndim, plan->sub_cap);
   PGB_REQUIRE(smem <= 227 * 1024, PGB_ERR_UNSUPPORTED, "%s: tile + staging need %zu B of shared memory", who, smem);
+  PGB_REQUIRE(plan->n_zero_bricks >= 0 && plan->n_empty_tail >= 0 && plan->n_empty_tail <= plan->n_zero_bricks,
+              PGB_ERR_INVALID, "%s: bad zero-brick counts", who);
+  PGB_REQUIRE(plan->n_zero_bricks == 0 || plan->zero_bricks != nullptr, PGB_ERR_INVALID, "%s: null zero-brick list",
+              who);
   cudaStream_t s = as_stream(stream);
-  if (plan->n_zero_bricks > 0) {
-    PGB_REQUIRE(plan->zero_bricks != nullptr, PGB_ERR_INVALID, "%s: null zero-brick list", who);
-    const int64_t tot = static_cast<int64_t>(plan->n_zero_bricks) * cells;
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  const bool tma = plan->n_cta > 0 && C == padded(C) && make_tile_map(&tmap, grid, plan, C, B);
+  // empty bricks at the end of the list are cleared by the gridding CTAs on
+  // the tensor-copy path; the rest (split bricks, which take reduce-adds) first
+  const int n_tail = tma ? plan->n_empty_tail : 0;
+  const int n_pre = plan->n_zero_bricks - n_tail;
+  if (n_pre > 0) {
+    const int64_t tot = static_cast<int64_t>(n_pre) * cells;
     zero_bricks_tc<<<grid_for(tot, 256, 148 * 16), 256, 0, s>>>(static_cast<float2*>(grid), G, static_cast<int>(C),
-                                                               static_cast<int>(B), plan->zero_bricks,
-                                                               plan->n_zero_bricks, geom);
+                                                               static_cast<int>(B), plan->zero_bricks, n_pre, geom);
     PGB_LAUNCH_CHECK(who);
   }
   if (plan->n_cta == 0) return PGB_OK;
   dim3 grd(plan->n_cta, static_cast<unsigned>(B));
-  CUtensorMap tmap;
-  memset(&tmap, 0, sizeof(tmap));
-  const bool tma = C == padded(C) && make_tile_map(&tmap, grid, plan, C, B);
   const size_t smem_k = tc_smem(C, cells, nsteps, ndim, plan->sub_cap, true, tma);
   const int key = padded(C) * 10 + static_cast<int>(ndim);
   switch (key) {
@@ -1185,7 +1235,7 @@ int pgb_grog_grid_tc(const void* data, int64_t N, void* grid, int64_t G, const v
                               static_cast<const float2*>(dtab), static_cast<int>(nsteps),                       \
                               reinterpret_cast<const int4*>(plan->sd), reinterpret_cast<const int2*>(plan->si),  \
                               plan->cta_ptr, plan->uniq, reinterpret_cast<const int2*>(plan->meta), plan->w,     \
-                              plan->sub_cap, geom, tmap);                                                       \
+                              plan->sub_cap, geom, tmap, plan->zero_bricks + n_pre, n_tail);                    \
   } break;
     PGB_TC_DISPATCH(X)
 #undef X

@@ -238,6 +238,32 @@ def test_tensor_core_32_coils_smooth_calibration(cuda, mode):
     assert rel_l2(out.reshape(1, C, -1), ref_a) < tol
 
 
+@pytest.mark.parametrize("B", [1, 2])
+def test_tensor_core_forward_writes_every_cell(cuda, B):
+    """The forward's CTAs clear the empty bricks themselves (tensor-copy path)
+    and the split bricks are cleared beforehand: gridding into a NaN-filled
+    buffer gives what gridding into a fresh one gives (up to the order of
+    the split bricks' reduce-adds).  The
+    spokes fill only the centre of the grid (one sample in a corner sets the
+    coordinate scale), so most bricks are empty and the central ones split."""
+    coords, calib, data = _random_case(3, 32, 40, 48, 12, 1.0, 2, "sphere", 1, seed=11, B=B)
+    coords = (coords * 0.3).astype(np.float32)
+    coords[0, 0, :] = 15.0
+    g = GrogInterpolator(shape=(32,) * 3, coords=coords, oversamp=1.0, kernel_width=2, device=cuda)
+    g.calc_interp_table(calib, lamda=0.01, precision=1)
+    g.gridder_mode = "tc"
+    kg = torch.as_tensor(np.asarray(g.grid(data))).to(cuda)
+    br = g._brick(0)
+    assert br._tile_copies() and br.plan.n_empty_tail > 0
+    G = int(np.prod(g.plan.grid_shape))
+    d = torch.as_tensor(np.asarray(data)).to(cuda).reshape(B, 12, -1).contiguous()
+    out = torch.full((B, 12, G), float("nan"), dtype=torch.complex64, device=cuda)
+    br.forward(d, out)
+    torch.cuda.synchronize()
+    assert bool(torch.isfinite(torch.view_as_real(out)).all())
+    assert rel_l2(out.cpu().numpy(), kg.reshape(B, 12, G).cpu().numpy()) < 1e-6
+
+
 def test_tensor_core_fallback_paths_match(cuda):
     """Odd grid width (no tensor copies of brick tiles) and the tensor copies
     switched off give the same operator as the default path."""

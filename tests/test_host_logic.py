@@ -197,6 +197,11 @@ def test_brick_plan6_invariants(shape, brick, n_outer, sub_cap):
     nb = int(np.prod(bp.nb))
     occupied = set(work[:, 0].tolist())
     assert set(bp.zero_bricks.numpy().tolist()) == (set(range(nb)) - occupied) | split_bricks
+    # split bricks first (cleared before the gridding kernel), the empty ones last
+    zb = bp.zero_bricks.numpy().tolist()
+    n_split = len(zb) - bp.n_empty_tail
+    assert set(zb[:n_split]) == split_bricks and set(zb[n_split:]) == set(range(nb)) - occupied
+    assert bp._c.n_empty_tail == bp.n_empty_tail and bp._c.n_zero_bricks == len(zb)
     # LPT keeps the CTAs balanced
     cost = bp.cta_cost
     assert cost.max() <= cost.mean() * 1.5 + (work[:, 2] - work[:, 1]).max() * sub_cap
