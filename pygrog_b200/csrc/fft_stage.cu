@@ -97,6 +97,7 @@ __global__ void fft_combine_kernel(const float2* __restrict__ v, const float2* _
     float2 acc = make_float2(0.f, 0.f);
     if (smaps) {
       const int64_t b = bc;
+#pragma unroll 4  // loads of four coils in flight per thread (c3 batch 131.9 against 134.0 ms)
       for (int c = 0; c < C; ++c)
         cfma_conj(acc, smaps[static_cast<int64_t>(c) * I + q], v[(b * C + c) * G + m]);
     } else {
