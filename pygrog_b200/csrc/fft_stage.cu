@@ -43,36 +43,42 @@ __device__ __forceinline__ int p2m(int p, int g) {
 }
 
 // u[b, c, m] = scale * S[c, q] * x[b, q]   (or x[b, c, q] without smaps)
-// for every FFT-order grid position m; zero outside the image.
+// for every FFT-order grid position m; zero outside the image.  One grid
+// row (b, c, m0, m1) per block step: the row is decoded once and its
+// threads run along x, so no element pays an integer division.
 __global__ void fft_expand_kernel(const float2* __restrict__ x, const float2* __restrict__ smaps,
                                   float2* __restrict__ u, int B, int C, Shape3 s, float scale,
                                   int x_has_coils) {
-  const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
   const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
-  const int64_t total = static_cast<int64_t>(B) * C * G;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t m = t % G;
-    const int64_t bc = t / G;
+  const int g2 = s.g[2];
+  const int64_t plane = static_cast<int64_t>(s.g[0]) * s.g[1];  // rows of one (b, c) grid
+  const int64_t rows = static_cast<int64_t>(B) * C * plane;
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int64_t bc = r / plane;
+    const int rem = static_cast<int>(r - bc * plane);
+    const int m0 = rem / s.g[1], m1 = rem - m0 * s.g[1];
     const int c = static_cast<int>(bc % C);
-    const int b = static_cast<int>(bc / C);
-    int m0, m1, m2;
-    unflat3(m, s.g, m0, m1, m2);
+    const int64_t b = bc / C;
     const int q0 = m2p(m0, s.g[0]) - s.off[0];
     const int q1 = m2p(m1, s.g[1]) - s.off[1];
-    const int q2 = m2p(m2, s.g[2]) - s.off[2];
-    float2 v = make_float2(0.f, 0.f);
-    if (q0 >= 0 && q0 < s.n[0] && q1 >= 0 && q1 < s.n[1] && q2 >= 0 && q2 < s.n[2]) {
-      const int64_t q = (static_cast<int64_t>(q0) * s.n[1] + q1) * s.n[2] + q2;
-      if (x_has_coils) {
-        v = x[(static_cast<int64_t>(b) * C + c) * I + q];
-      } else {
-        v = x[static_cast<int64_t>(b) * I + q];
-        if (smaps) v = cmul(v, smaps[static_cast<int64_t>(c) * I + q]);
-      }
-      v = cscale(v, scale);
+    float2* urow = u + r * g2;
+    if (q0 < 0 || q0 >= s.n[0] || q1 < 0 || q1 >= s.n[1]) {  // block-uniform: a padding row
+      for (int m2 = threadIdx.x; m2 < g2; m2 += blockDim.x) urow[m2] = make_float2(0.f, 0.f);
+      continue;
     }
-    u[t] = v;
+    const int64_t qrow = (static_cast<int64_t>(q0) * s.n[1] + q1) * s.n[2];
+    const float2* xrow = x + (x_has_coils ? (b * C + c) * I : b * I) + qrow;
+    const float2* srow = smaps ? smaps + static_cast<int64_t>(c) * I + qrow : nullptr;
+    for (int m2 = threadIdx.x; m2 < g2; m2 += blockDim.x) {
+      const int q2 = m2p(m2, g2) - s.off[2];
+      float2 v = make_float2(0.f, 0.f);
+      if (q2 >= 0 && q2 < s.n[2]) {
+        v = xrow[q2];
+        if (!x_has_coils && smaps) v = cmul(v, srow[q2]);
+        v = cscale(v, scale);
+      }
+      urow[m2] = v;
+    }
   }
 }
 
@@ -156,12 +162,21 @@ __global__ void sparse_gather_kernel(const float2* __restrict__ U, const int32_t
   }
 }
 
-// U[bc, m] *= psf[m]  (real point-spread function in FFT order)
+// U[bc, m] *= psf[m]  (real point-spread function in FFT order): a thread
+// per position m reads psf[m] once and scales it in kPsfRows planes
+// bc = blockIdx.y * kPsfRows + j (no per-element modulo).
+constexpr int kPsfRows = 4;
 __global__ void psf_apply_kernel(float2* __restrict__ U, const float* __restrict__ psf, int BC, int64_t G) {
-  const int64_t total = static_cast<int64_t>(BC) * G;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    U[t] = cscale(U[t], psf[t % G]);
+  const int bc0 = blockIdx.y * kPsfRows;
+  const int nb = min(kPsfRows, BC - bc0);
+  for (int64_t m = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; m < G;
+       m += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float w = psf[m];
+    float2* col = U + static_cast<int64_t>(bc0) * G + m;
+#pragma unroll
+    for (int j = 0; j < kPsfRows; ++j)
+      if (j < nb) col[j * G] = cscale(col[j * G], w);
+  }
 }
 
 // dst[bc, m] = scale * mask[p(m)] * src[bc, p(m)]   (centred -> FFT order)
@@ -226,7 +241,8 @@ int pgb_fft_expand(const void* x, const void* smaps, void* u, int64_t B, int64_t
   if (B == 0) return PGB_OK;
   PGB_REQUIRE(x && u, PGB_ERR_INVALID, "fft_expand: null pointer");
   const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
-  fft_expand_kernel<<<grid_for(B * C * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+  const int64_t rows = B * C * G / s.g[2];
+  fft_expand_kernel<<<static_cast<int>(rows < 148 * 64 ? rows : 148 * 64), 128, 0, as_stream(stream)>>>(
       static_cast<const float2*>(x), static_cast<const float2*>(smaps), static_cast<float2*>(u),
       static_cast<int>(B), static_cast<int>(C), s, scale, x_has_coils);
   PGB_LAUNCH_CHECK("fft_expand");
@@ -280,8 +296,9 @@ int pgb_psf_apply(void* U, const float* psf, int64_t BC, int64_t G, void* stream
   PGB_REQUIRE(BC >= 0 && G >= 0, PGB_ERR_INVALID, "psf_apply: negative size");
   if (BC == 0 || G == 0) return PGB_OK;
   PGB_REQUIRE(U && psf, PGB_ERR_INVALID, "psf_apply: null pointer");
-  psf_apply_kernel<<<grid_for(BC * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(static_cast<float2*>(U),
-                                                                                psf, static_cast<int>(BC), G);
+  PGB_REQUIRE(BC <= 65535 * static_cast<int64_t>(kPsfRows), PGB_ERR_RANGE, "psf_apply: too many planes");
+  const dim3 grd(grid_for(G, 256, 148 * 32), static_cast<unsigned>((BC + kPsfRows - 1) / kPsfRows));
+  psf_apply_kernel<<<grd, 256, 0, as_stream(stream)>>>(static_cast<float2*>(U), psf, static_cast<int>(BC), G);
   PGB_LAUNCH_CHECK("psf_apply");
   return PGB_OK;
 }
