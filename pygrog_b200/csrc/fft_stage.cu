@@ -24,13 +24,6 @@ struct Shape3 {
   int off[3];    // (g - n) / 2 : image origin inside the centred grid
 };
 
-__device__ __forceinline__ void unflat3(int64_t t, const int* e, int& a, int& b, int& c) {
-  c = static_cast<int>(t % e[2]);
-  const int64_t u = t / e[2];
-  b = static_cast<int>(u % e[1]);
-  a = static_cast<int>(u / e[1]);
-}
-
 // FFT-order index m -> centred index p (per axis)
 __device__ __forceinline__ int m2p(int m, int g) {
   int p = m + g / 2;
@@ -85,80 +78,90 @@ __global__ void fft_expand_kernel(const float2* __restrict__ x, const float2* __
 // out[b, q] = scale * sum_c conj(S[c, q]) v[b, c, m(q)]   (smaps)
 // out[b, c, q] = scale * v[b, c, m(q)]                      (no smaps)
 // optionally + add_scale * add[b, (c,) q]  (damped normal equations).
+// One output per thread: image row r = (b, (c,) q0, q1) from blockIdx.y
+// (grid-stride) and threadIdx.y, q2 from blockIdx.x and threadIdx.x, so the
+// only divisions are the row's.
 __global__ void fft_combine_kernel(const float2* __restrict__ v, const float2* __restrict__ smaps,
                                    float2* __restrict__ out, int B, int C, Shape3 s, float scale,
                                    const float2* __restrict__ add, float add_scale) {
   const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
   const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
-  const int Cout = smaps ? 1 : C;
-  const int64_t total = static_cast<int64_t>(B) * Cout * I;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t q = t % I;
-    const int64_t bc = t / I;
-    int q0, q1, q2;
-    unflat3(q, s.n, q0, q1, q2);
-    const int64_t m = (static_cast<int64_t>(p2m(q0 + s.off[0], s.g[0])) * s.g[1] +
-                       p2m(q1 + s.off[1], s.g[1])) * s.g[2] + p2m(q2 + s.off[2], s.g[2]);
-    float2 acc = make_float2(0.f, 0.f);
-    if (smaps) {
-      const int64_t b = bc;
-#pragma unroll 4  // loads of four coils in flight per thread (c3 batch 131.9 against 134.0 ms)
-      for (int c = 0; c < C; ++c)
-        cfma_conj(acc, smaps[static_cast<int64_t>(c) * I + q], v[(b * C + c) * G + m]);
-    } else {
-      acc = v[bc * G + m];
+  const int n2 = s.n[2];
+  const int q2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q2 >= n2) return;
+  const int64_t plane = static_cast<int64_t>(s.n[0]) * s.n[1];  // image rows of one output plane
+  const int64_t rows = static_cast<int64_t>(B) * (smaps ? 1 : C) * plane;
+  for (int64_t r = static_cast<int64_t>(blockIdx.y) * blockDim.y + threadIdx.y; r < rows;
+       r += static_cast<int64_t>(gridDim.y) * blockDim.y) {
+    const int64_t bc = r / plane;  // frame (smaps) or frame * C + coil
+    const int rem = static_cast<int>(r - bc * plane);
+    const int q0 = rem / s.n[1], q1 = rem - q0 * s.n[1];
+    const int64_t qrow = static_cast<int64_t>(rem) * n2;
+    {
+      const int64_t m = (static_cast<int64_t>(p2m(q0 + s.off[0], s.g[0])) * s.g[1] +
+                         p2m(q1 + s.off[1], s.g[1])) * s.g[2] + p2m(q2 + s.off[2], s.g[2]);
+      float2 acc = make_float2(0.f, 0.f);
+      if (smaps) {
+#pragma unroll 4  // loads of four coils in flight per thread
+        for (int c = 0; c < C; ++c)
+          cfma_conj(acc, smaps[static_cast<int64_t>(c) * I + qrow + q2], v[(bc * C + c) * G + m]);
+      } else {
+        acc = v[bc * G + m];
+      }
+      acc = cscale(acc, scale);
+      const int64_t t = r * n2 + q2;
+      if (add) {
+        const float2 a = add[t];
+        acc.x = fmaf(add_scale, a.x, acc.x);
+        acc.y = fmaf(add_scale, a.y, acc.y);
+      }
+      out[t] = acc;
     }
-    acc = cscale(acc, scale);
-    if (add) {
-      const float2 a = add[t];
-      acc.x = fmaf(add_scale, a.x, acc.x);
-      acc.y = fmaf(add_scale, a.y, acc.y);
-    }
-    out[t] = acc;
   }
 }
 
 // u[b, c, cellpos[r]] += w[r] * data[b, c, r]  (warp-aggregated atomics; u zeroed by caller)
+// plane bc = b * C + c in y (grid-stride), replicas r in x
 __global__ void __launch_bounds__(256) sparse_scatter_kernel(const float2* __restrict__ data,
                                                              const int32_t* __restrict__ cellpos,
                                                              const float* __restrict__ w,
                                                              float2* __restrict__ u, int BC, int64_t R,
                                                              int64_t G) {
-  const int64_t total = static_cast<int64_t>(BC) * R;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < total; base += stride) {
-    const int64_t t = base + threadIdx.x;
-    int64_t key = -1;
-    float2 val = make_float2(0.f, 0.f);
-    if (t < total) {
-      const int64_t r = t % R;
-      const int64_t bc = t / R;
-      const int32_t cp = cellpos[r];
-      const float ww = w[r];
-      if (cp >= 0 && cp < G && ww != 0.f) {
-        key = bc * G + cp;
-        val = cscale(data[t], ww);
+  for (int bc = blockIdx.y; bc < BC; bc += gridDim.y) {
+    const float2* drow = data + static_cast<int64_t>(bc) * R;
+    for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < R; base += stride) {
+      const int64_t r = base + threadIdx.x;
+      int64_t key = -1;
+      float2 val = make_float2(0.f, 0.f);
+      if (r < R) {
+        const int32_t cp = cellpos[r];
+        const float ww = w[r];
+        if (cp >= 0 && cp < G && ww != 0.f) {
+          key = static_cast<int64_t>(bc) * G + cp;
+          val = cscale(drow[r], ww);
+        }
       }
+      const unsigned active = __ballot_sync(0xffffffffu, key >= 0);
+      if (key >= 0) warp_aggregated_add(u, key, val, active);
     }
-    const unsigned active = __ballot_sync(0xffffffffu, key >= 0);
-    if (key >= 0) warp_aggregated_add(u, key, val, active);
   }
 }
 
-// out[b, c, r] = w[r] * U[b, c, cellpos[r]]
+// out[b, c, r] = w[r] * U[b, c, cellpos[r]]   (plane bc in y, replicas r in x)
 __global__ void sparse_gather_kernel(const float2* __restrict__ U, const int32_t* __restrict__ cellpos,
                                      const float* __restrict__ w, float2* __restrict__ out, int BC,
                                      int64_t R, int64_t G) {
-  const int64_t total = static_cast<int64_t>(BC) * R;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t r = t % R;
-    const int64_t bc = t / R;
-    const int32_t cp = cellpos[r];
-    float2 v = make_float2(0.f, 0.f);
-    if (cp >= 0 && cp < G) v = cscale(U[bc * G + cp], w[r]);
-    out[t] = v;
+  for (int bc = blockIdx.y; bc < BC; bc += gridDim.y) {
+    const float2* Ub = U + static_cast<int64_t>(bc) * G;
+    float2* ob = out + static_cast<int64_t>(bc) * R;
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < R;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const int32_t cp = cellpos[r];
+      float2 v = make_float2(0.f, 0.f);
+      if (cp >= 0 && cp < G) v = cscale(Ub[cp], w[r]);
+      ob[r] = v;
+    }
   }
 }
 
@@ -181,25 +184,29 @@ __global__ void psf_apply_kernel(float2* __restrict__ U, const float* __restrict
 
 // dst[bc, m] = scale * mask[p(m)] * src[bc, p(m)]   (centred -> FFT order)
 // dst[bc, p] = scale * mask[p] * src[bc, m(p)]      (FFT order -> centred), to_centred = 1
+// Grid rows (bc, i0, i1): threadIdx.y picks one of blockDim.y rows per block
+// step, decoded once; the x threads run along the last axis.
 __global__ void fft_shift_kernel(const float2* __restrict__ src, const float* __restrict__ mask,
                                  float2* __restrict__ dst, int BC, Shape3 s, float scale, int to_centred) {
   const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
-  const int64_t total = static_cast<int64_t>(BC) * G;
-  for (int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = t % G;
-    const int64_t bc = t / G;
-    int a0, a1, a2;
-    unflat3(i, s.g, a0, a1, a2);
-    int64_t j;
-    if (to_centred) {
-      j = (static_cast<int64_t>(p2m(a0, s.g[0])) * s.g[1] + p2m(a1, s.g[1])) * s.g[2] + p2m(a2, s.g[2]);
-      const float mk = mask ? mask[i] : 1.f;
-      dst[t] = cscale(src[bc * G + j], scale * mk);
-    } else {
-      j = (static_cast<int64_t>(m2p(a0, s.g[0])) * s.g[1] + m2p(a1, s.g[1])) * s.g[2] + m2p(a2, s.g[2]);
-      const float mk = mask ? mask[j] : 1.f;
-      dst[t] = cscale(src[bc * G + j], scale * mk);
+  const int g2 = s.g[2];
+  const int64_t plane = static_cast<int64_t>(s.g[0]) * s.g[1];
+  const int64_t rows = static_cast<int64_t>(BC) * plane;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.y + threadIdx.y; r < rows;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.y) {
+    const int64_t bc = r / plane;
+    const int rem = static_cast<int>(r - bc * plane);
+    const int a0 = rem / s.g[1], a1 = rem - a0 * s.g[1];
+    const int64_t irow = static_cast<int64_t>(rem) * g2;  // this row within the plane
+    const int64_t jrow = to_centred
+                             ? (static_cast<int64_t>(p2m(a0, s.g[0])) * s.g[1] + p2m(a1, s.g[1])) * g2
+                             : (static_cast<int64_t>(m2p(a0, s.g[0])) * s.g[1] + m2p(a1, s.g[1])) * g2;
+    const float2* srow = src + bc * G + jrow;
+    float2* drow = dst + r * g2;
+    for (int a2 = threadIdx.x; a2 < g2; a2 += blockDim.x) {
+      const int j2 = to_centred ? p2m(a2, g2) : m2p(a2, g2);
+      const float mk = mask ? mask[to_centred ? irow + a2 : jrow + j2] : 1.f;
+      drow[a2] = cscale(srow[j2], scale * mk);
     }
   }
 }
@@ -260,7 +267,9 @@ int pgb_fft_combine(const void* v, const void* smaps, void* out, int64_t B, int6
   if (B == 0) return PGB_OK;
   PGB_REQUIRE(v && out, PGB_ERR_INVALID, "fft_combine: null pointer");
   const int64_t I = static_cast<int64_t>(s.n[0]) * s.n[1] * s.n[2];
-  fft_combine_kernel<<<grid_for(B * (smaps ? 1 : C) * I, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+  const int64_t rows = B * (smaps ? 1 : C) * I / s.n[2];
+  const dim3 grd((s.n[2] + 31) / 32, static_cast<unsigned>(grid_for(rows, 8, 65535)));
+  fft_combine_kernel<<<grd, dim3(32, 8), 0, as_stream(stream)>>>(
       static_cast<const float2*>(v), static_cast<const float2*>(smaps), static_cast<float2*>(out),
       static_cast<int>(B), static_cast<int>(C), s, scale, static_cast<const float2*>(add), add_scale);
   PGB_LAUNCH_CHECK("fft_combine");
@@ -273,7 +282,9 @@ int pgb_sparse_scatter(const void* data, const int32_t* cellpos, const float* w,
   PGB_REQUIRE(BC >= 0 && R >= 0 && G >= 0, PGB_ERR_INVALID, "sparse_scatter: negative size");
   if (BC == 0 || R == 0 || G == 0) return PGB_OK;
   PGB_REQUIRE(data && cellpos && w && u, PGB_ERR_INVALID, "sparse_scatter: null pointer");
-  sparse_scatter_kernel<<<grid_for(BC * R, 256, 148 * 16), 256, 0, as_stream(stream)>>>(
+  const unsigned ys = static_cast<unsigned>(BC < 65535 ? BC : 65535);
+  const int xs = grid_for(R, 256, (148 * 16 + ys - 1) / ys);
+  sparse_scatter_kernel<<<dim3(xs, ys), 256, 0, as_stream(stream)>>>(
       static_cast<const float2*>(data), cellpos, w, static_cast<float2*>(u), static_cast<int>(BC), R, G);
   PGB_LAUNCH_CHECK("sparse_scatter");
   return PGB_OK;
@@ -285,7 +296,9 @@ int pgb_sparse_gather(const void* U, const int32_t* cellpos, const float* w, voi
   PGB_REQUIRE(BC >= 0 && R >= 0 && G >= 0, PGB_ERR_INVALID, "sparse_gather: negative size");
   if (BC == 0 || R == 0) return PGB_OK;
   PGB_REQUIRE(U && cellpos && w && out, PGB_ERR_INVALID, "sparse_gather: null pointer");
-  sparse_gather_kernel<<<grid_for(BC * R, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+  const unsigned ys = static_cast<unsigned>(BC < 65535 ? BC : 65535);
+  const int xs = grid_for(R, 256, (148 * 32 + ys - 1) / ys);
+  sparse_gather_kernel<<<dim3(xs, ys), 256, 0, as_stream(stream)>>>(
       static_cast<const float2*>(U), cellpos, w, static_cast<float2*>(out), static_cast<int>(BC), R, G);
   PGB_LAUNCH_CHECK("sparse_gather");
   return PGB_OK;
@@ -313,7 +326,7 @@ int pgb_fft_shift(const void* src, const float* mask, void* dst, int64_t BC, int
   if (BC == 0) return PGB_OK;
   PGB_REQUIRE(src && dst && src != dst, PGB_ERR_INVALID, "fft_shift: null or aliased pointers");
   const int64_t G = static_cast<int64_t>(s.g[0]) * s.g[1] * s.g[2];
-  fft_shift_kernel<<<grid_for(BC * G, 256, 148 * 32), 256, 0, as_stream(stream)>>>(
+  fft_shift_kernel<<<grid_for(BC * G / s.g[2], 4, 148 * 64), dim3(64, 4), 0, as_stream(stream)>>>(
       static_cast<const float2*>(src), mask, static_cast<float2*>(dst), static_cast<int>(BC), s, scale,
       to_centred);
   PGB_LAUNCH_CHECK("fft_shift");
